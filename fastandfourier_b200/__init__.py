@@ -1,0 +1,252 @@
+"""fastandfourier_b200 -- B200 (sm_100a) implementation of FastAndFourier's
+batched split-plane transform path behind the reference's C API.
+
+The product is the C-ABI library libfaf_b200.so (include/fastandfourier.h,
+include/chirp.h, include/faf_cuda.h).  This package is its Python host
+mirror: `Transform` wraps one faf_transform * and runs it on torch CUDA
+tensors (device pointers, on the current torch stream) or on numpy arrays
+(host pointers, copied in and out by the library).  The operation names
+follow the reference API (faf_create_fft / faf_create_rfft /
+faf_create_stft / chirp_compile / chirp_bind / faf_execute).
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _lib as C
+from ._lib import (B_CUDA, DIR_FORWARD, DIR_INVERSE, FLAG_BLUESTEIN, FLAG_MEASURE,
+                   L_DEFAULT, L_HERMITIAN, L_INTERLEAVED, L_REAL, L_SPLIT, N_DEFAULT,
+                   N_FORWARD, N_NONE, N_ORTHO, T_FFT, T_IFFT, T_IRFFT, T_PIPELINE, T_RFFT,
+                   T_STFT)
+
+__all__ = ["FafError", "Transform", "config", "lib", "available", "B_CUDA", "DIR_FORWARD",
+           "DIR_INVERSE", "FLAG_BLUESTEIN", "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
+           "L_INTERLEAVED", "L_REAL", "L_SPLIT", "N_DEFAULT", "N_FORWARD", "N_NONE", "N_ORTHO",
+           "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
+
+
+class FafError(RuntimeError):
+    """A create / execute call of libfaf_b200.so failed (message from
+    faf_get_error())."""
+
+
+def lib():
+    return C.lib()
+
+
+def available():
+    return bool(C.lib().faf_cuda_available())
+
+
+def config(n, *, dir=DIR_FORWARD, norm=N_DEFAULT, layout=L_DEFAULT, flags=0, hop=0, win=0,
+           backend=0):
+    c = C.faf_config()
+    c.n = n
+    c.precision = C.PREC_FP32
+    c.dir = dir
+    c.norm = norm
+    c.layout = layout
+    c.flags = flags
+    c.hop_length = hop
+    c.win_length = win
+    c.backend = backend
+    return c
+
+
+def _ptr(a):
+    """Raw data pointer of a torch tensor or numpy array (must be float32 and
+    contiguous)."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        if not a.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return a.data_ptr()
+    if hasattr(a, "ctypes"):
+        if not a.flags["C_CONTIGUOUS"]:
+            raise ValueError("array must be C-contiguous")
+        return a.ctypes.data
+    raise TypeError(f"unsupported buffer type {type(a)!r}")
+
+
+def _buf(re, im, n, layout):
+    b = C.faf_buffer()
+    b.re = _ptr(re)
+    b.im = _ptr(im)
+    b.n = n
+    b.layout = layout
+    return b
+
+
+def _check(rc):
+    if rc != 0:
+        raise FafError(C.error())
+
+
+def _empty_like_batch(ref, shape):
+    if hasattr(ref, "data_ptr"):
+        import torch
+        return torch.empty(shape, dtype=torch.float32, device=ref.device)
+    import numpy as np
+    return np.empty(shape, np.float32)
+
+
+class Transform:
+    """One faf_transform * of libfaf_b200.so."""
+
+    def __init__(self, ptr, keep=()):
+        if not ptr:
+            raise FafError(C.error())
+        self._p = ptr
+        self._keep = list(keep)
+
+    # ---- constructors (reference names) ----
+    @classmethod
+    def fft(cls, n, *, inverse=False, norm=N_DEFAULT, layout=L_DEFAULT, flags=0):
+        c = config(n, dir=DIR_INVERSE if inverse else DIR_FORWARD, norm=norm, layout=layout,
+                   flags=flags)
+        return cls(C.lib().faf_create_fft(ctypes.byref(c)))
+
+    @classmethod
+    def rfft(cls, n, *, inverse=False, norm=N_DEFAULT, layout=L_DEFAULT):
+        c = config(n, dir=DIR_INVERSE if inverse else DIR_FORWARD, norm=norm, layout=layout)
+        return cls(C.lib().faf_create_rfft(ctypes.byref(c)))
+
+    @classmethod
+    def stft(cls, n, *, win=0, hop=0):
+        c = config(n, hop=hop, win=win)
+        return cls(C.lib().faf_create_stft(ctypes.byref(c)))
+
+    @classmethod
+    def chirp(cls, source):
+        return cls(C.lib().chirp_compile(source.encode()))
+
+    def inverse(self):
+        return Transform(C.lib().faf_create_inverse(self._p))
+
+    # ---- fields ----
+    @property
+    def ptr(self):
+        return self._p
+
+    @property
+    def s(self):
+        return self._p.contents
+
+    @property
+    def n(self):
+        return self.s.n
+
+    @property
+    def type(self):
+        return self.s.type
+
+    @property
+    def kind(self):
+        k = C.lib().faf_cuda_plan_kind(self._p)
+        return k.decode() if k else None
+
+    def spectrum_len(self):
+        return C.lib().faf_spectrum_len(self._p)
+
+    # ---- binding / streams ----
+    def bind(self, hr, hi, n_bins=None, name="H"):
+        n_bins = n_bins if n_bins is not None else len(hr)
+        self._keep += [hr, hi]
+        _check(C.lib().chirp_bind(self._p, name.encode(), _ptr(hr), _ptr(hi), n_bins))
+
+    def set_stream(self, stream):
+        """stream: torch.cuda.Stream, a raw cudaStream_t int, or None."""
+        h = getattr(stream, "cuda_stream", stream)
+        _check(C.lib().faf_cuda_set_stream(self._p, h or None))
+
+    def synchronize(self):
+        _check(C.lib().faf_cuda_synchronize(self._p))
+
+    # ---- execute ----
+    def execute(self, out, inp):
+        """faf_execute with two faf_buffer descriptors."""
+        _check(C.lib().faf_execute(self._p, ctypes.byref(out), ctypes.byref(inp)))
+
+    def execute_batched(self, out, inp, batch, in_dist=0, out_dist=0):
+        _check(C.lib().faf_execute_batched(self._p, ctypes.byref(out), ctypes.byref(inp),
+                                           batch, in_dist, out_dist))
+
+    def c2c(self, re, im=None, out_re=None, out_im=None):
+        """Batched C2C over the last axis.  Split planes (re, im) or one
+        interleaved buffer (re only, shape (..., 2n)) for INTERLEAVED plans."""
+        n = self.n
+        inter = self.s.cfg.layout == L_INTERLEAVED
+        lay = L_INTERLEAVED if inter else L_SPLIT
+        batch = (re.numel() if hasattr(re, "numel") else re.size) // (2 * n if inter else n)
+        if out_re is None:
+            out_re = _empty_like_batch(re, tuple(re.shape))
+            out_im = None if inter else _empty_like_batch(re, tuple(re.shape))
+        self.execute_batched(_buf(out_re, out_im, n, lay), _buf(re, im, n, lay), batch)
+        return out_re if inter else (out_re, out_im)
+
+    def r2c(self, x, out_re=None, out_im=None):
+        n, nb = self.n, self.n // 2 + 1
+        batch = (x.numel() if hasattr(x, "numel") else x.size) // n
+        shp = tuple(x.shape[:-1]) + (nb,)
+        inter = self.s.cfg.layout == L_INTERLEAVED
+        if out_re is None:
+            out_re = _empty_like_batch(x, shp + (2,) if inter else shp)
+            out_im = None if inter else _empty_like_batch(x, shp)
+        lay = L_INTERLEAVED if inter else L_HERMITIAN
+        self.execute_batched(_buf(out_re, out_im, nb, lay), _buf(x, None, n, L_REAL), batch)
+        return out_re if inter else (out_re, out_im)
+
+    def c2r(self, Xr, Xi=None, out=None):
+        n, nb = self.n, self.n // 2 + 1
+        inter = self.s.cfg.layout == L_INTERLEAVED
+        cnt = Xr.numel() if hasattr(Xr, "numel") else Xr.size
+        batch = cnt // (2 * nb if inter else nb)
+        shp = (tuple(Xr.shape[:-2]) if inter else tuple(Xr.shape[:-1])) + (n,)
+        if out is None:
+            out = _empty_like_batch(Xr, shp)
+        lay = L_INTERLEAVED if inter else L_HERMITIAN
+        self.execute_batched(_buf(out, None, n, L_REAL), _buf(Xr, Xi, nb, lay), batch)
+        return out
+
+    def pipeline(self, x, out=None):
+        n = self.n
+        batch = (x.numel() if hasattr(x, "numel") else x.size) // n
+        if out is None:
+            out = _empty_like_batch(x, tuple(x.shape))
+        self.execute_batched(_buf(out, None, n, L_REAL), _buf(x, None, n, L_REAL), batch)
+        return out
+
+    def frames(self, sig_len):
+        win, hop = self.s.win_length, self.s.hop_length
+        return 1 + (sig_len - win) // hop
+
+    def stft_frames(self, x, out_re=None, out_im=None):
+        """Framed real STFT of signals x (n_sig, L) -> (n_sig, F, n/2+1)."""
+        L = x.shape[-1]
+        n_sig = (x.numel() if hasattr(x, "numel") else x.size) // L
+        F, nb = self.frames(L), self.n // 2 + 1
+        shp = tuple(x.shape[:-1]) + (F, nb)
+        if out_re is None:
+            out_re = _empty_like_batch(x, shp)
+            out_im = _empty_like_batch(x, shp)
+        self.execute_batched(_buf(out_re, out_im, F * nb, L_HERMITIAN),
+                             _buf(x, None, L, L_REAL), n_sig)
+        return out_re, out_im
+
+    def close(self):
+        if self._p:
+            C.lib().faf_destroy_transform(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

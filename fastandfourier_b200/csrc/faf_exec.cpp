@@ -1,0 +1,455 @@
+// faf_exec.cpp -- faf_execute / faf_execute_batched: buffer validation (the
+// reference's rules, src/faf_core.c:1298-1367, src/faf_rfft.c:268-335,
+// src/faf_pipeline.c:10-60), host/device memory detection and staging, and
+// dispatch to the kernels of each plan kind.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "chirp.h"
+#include "faf_api_internal.h"
+#include "faf_cuda.h"
+
+using fafp::DevicePlan;
+using fafp::Kind;
+using namespace fafapi;
+
+namespace {
+
+// One plane region of a (possibly batched, strided) buffer.
+struct Region {
+    const void* src;   // caller pointer (input) or NULL
+    void* dst;         // caller pointer (output) or NULL
+    size_t floats;     // floats spanned
+};
+
+size_t span_floats(long long batch, long long dist, size_t len, int fpe) {
+    if (batch <= 0) return 0;
+    return ((size_t)(batch - 1) * (size_t)dist + len) * (size_t)fpe;
+}
+
+// What one execute needs from the buffers, after validation.
+struct Request {
+    const float* in_a = nullptr;
+    const float* in_b = nullptr;
+    float* out_a = nullptr;
+    float* out_b = nullptr;
+    size_t in_len = 0, out_len = 0;   // elements per plane per transform
+    int in_fpe = 1, out_fpe = 1;      // floats per element (2 = interleaved)
+    long long batch = 1, in_dist = 0, out_dist = 0;
+    bool interleaved = false;         // complex side interleaved
+    bool framed = false;              // STFT: framed real signal
+    long long frames = 0, sig_len = 0;
+};
+
+int check_layouts_c2c(const faf_transform* t, const faf_buffer* out, const faf_buffer* in,
+                      Request& r) {
+    if (in->layout != t->cfg.layout || out->layout != t->cfg.layout)
+        return fail("buffer layout (%s/%s) does not match transform (%s)",
+                    faf_layout_name(in->layout), faf_layout_name(out->layout),
+                    faf_layout_name(t->cfg.layout));
+    if (!in->re || !out->re) return fail("execute buffers must provide re");
+    const bool inter = t->cfg.layout == FAF_LAYOUT_INTERLEAVED;
+    if (!inter && (!in->im || !out->im))
+        return fail("split/hermitian layout requires im planes");
+    if ((t->flags & FAF_FLAG_BLUESTEIN) && (in->n != t->n || out->n != t->n))
+        return fail("bluestein: buffer length must be %zu", t->n);
+    if (in->n < t->n || out->n < t->n)
+        return fail("execute buffers hold %zu/%zu elements, transform needs %zu", in->n, out->n,
+                    t->n);
+    r.interleaved = inter;
+    r.in_a = (const float*)in->re;
+    r.in_b = inter ? nullptr : (const float*)in->im;
+    r.out_a = (float*)out->re;
+    r.out_b = inter ? nullptr : (float*)out->im;
+    r.in_len = r.out_len = t->n;
+    r.in_fpe = r.out_fpe = inter ? 2 : 1;
+    return 0;
+}
+
+int check_rfft(const faf_transform* t, const faf_buffer* out, const faf_buffer* in, Request& r) {
+    if (!in->re || !out->re) return fail("execute buffers must provide re");
+    const bool inverse = t->type == FAF_TRANSFORM_IRFFT || t->cfg.dir == FAF_DIR_INVERSE;
+    const size_t n = t->n, nb = n / 2 + 1;
+    const faf_layout spec = t->cfg.layout;
+    const bool inter = spec == FAF_LAYOUT_INTERLEAVED;
+    if (!inverse) {
+        if (in->layout != FAF_LAYOUT_REAL)
+            return fail("rfft input must be REAL, got %s", faf_layout_name(in->layout));
+        if (in->n != n) return fail("rfft input n=%zu, expected %zu", in->n, n);
+        if (out->layout != spec)
+            return fail("rfft output layout (%s) does not match transform (%s)",
+                        faf_layout_name(out->layout), faf_layout_name(spec));
+        if (out->n != nb) return fail("rfft output n=%zu, expected %zu bins", out->n, nb);
+        if (spec == FAF_LAYOUT_HERMITIAN && !out->im)
+            return fail("hermitian rfft output requires im");
+        r.in_a = (const float*)in->re;
+        r.out_a = (float*)out->re;
+        r.out_b = inter ? nullptr : (float*)out->im;
+        r.in_len = n;
+        r.out_len = nb;
+        r.out_fpe = inter ? 2 : 1;
+    } else {
+        if (in->layout != spec)
+            return fail("irfft input layout (%s) does not match transform (%s)",
+                        faf_layout_name(in->layout), faf_layout_name(spec));
+        if (in->n != nb) return fail("irfft input n=%zu, expected %zu bins", in->n, nb);
+        if (spec == FAF_LAYOUT_HERMITIAN && !in->im)
+            return fail("hermitian irfft input requires im");
+        if (out->layout != FAF_LAYOUT_REAL)
+            return fail("irfft output must be REAL, got %s", faf_layout_name(out->layout));
+        if (out->n != n) return fail("irfft output n=%zu, expected %zu", out->n, n);
+        r.in_a = (const float*)in->re;
+        r.in_b = inter ? nullptr : (const float*)in->im;
+        r.out_a = (float*)out->re;
+        r.in_len = nb;
+        r.out_len = n;
+        r.in_fpe = inter ? 2 : 1;
+    }
+    r.interleaved = inter;
+    return 0;
+}
+
+int check_pipeline(const faf_transform* t, const faf_buffer* out, const faf_buffer* in,
+                   Request& r) {
+    const size_t n = t->n, nb = n / 2 + 1;
+    if (in->layout != FAF_LAYOUT_REAL || in->n != n || !in->re)
+        return fail("pipeline input must be REAL of length %zu", n);
+    r.in_a = (const float*)in->re;
+    r.in_len = n;
+    if (t->inner_inv) {
+        if (out->layout != FAF_LAYOUT_REAL || out->n != n || !out->re)
+            return fail("pipeline output must be REAL of length %zu", n);
+        r.out_a = (float*)out->re;
+        r.out_len = n;
+    } else {
+        if (out->layout != FAF_LAYOUT_HERMITIAN || out->n != nb || !out->re || !out->im)
+            return fail("analysis pipeline output must be HERMITIAN (%zu bins)", nb);
+        r.out_a = (float*)out->re;
+        r.out_b = (float*)out->im;
+        r.out_len = nb;
+    }
+    return 0;
+}
+
+int check_stft(const faf_transform* t, const faf_buffer* out, const faf_buffer* in,
+               Request& r) {
+    if (!in->re || !out->re) return fail("execute buffers must provide re");
+    const size_t n = t->n, nb = n / 2 + 1, win = t->win_length, hop = t->hop_length;
+    if (in->layout == FAF_LAYOUT_REAL) {
+        // Framed real STFT: F = 1 + (L - win) / hop frames of n/2+1 bins.
+        if (!t->inner || !plan_of(t->inner))
+            return fail("STFT framing needs an even 5-smooth FFT size, got %zu", n);
+        if (in->n < win) return fail("STFT signal length %zu shorter than window %zu", in->n, win);
+        const size_t F = 1 + (in->n - win) / hop;
+        const bool inter = out->layout == FAF_LAYOUT_INTERLEAVED;
+        if (out->layout != FAF_LAYOUT_HERMITIAN && !inter)
+            return fail("STFT output must be HERMITIAN (frames x %zu bins), got %s", nb,
+                        faf_layout_name(out->layout));
+        if (out->n != F * nb)
+            return fail("STFT output n=%zu, expected %zu frames x %zu bins = %zu", out->n, F, nb,
+                        F * nb);
+        if (!inter && !out->im) return fail("hermitian STFT output requires im");
+        r.framed = true;
+        r.frames = (long long)F;
+        r.sig_len = (long long)in->n;
+        r.in_a = (const float*)in->re;
+        r.out_a = (float*)out->re;
+        r.out_b = inter ? nullptr : (float*)out->im;
+        r.in_len = in->n;
+        r.out_len = F * nb;
+        r.out_fpe = inter ? 2 : 1;
+        r.interleaved = inter;
+        return 0;
+    }
+    // One windowed C2C frame of n (reference semantics, window applied on
+    // every complex layout).
+    if (in->layout != out->layout ||
+        (in->layout != FAF_LAYOUT_SPLIT && in->layout != FAF_LAYOUT_INTERLEAVED))
+        return fail("STFT frame buffers must both be SPLIT or INTERLEAVED");
+    faf_transform tmp = *t;
+    tmp.cfg.layout = in->layout;
+    tmp.flags &= ~FAF_FLAG_BLUESTEIN;
+    return check_layouts_c2c(&tmp, out, in, r);
+}
+
+// ---- memory staging -------------------------------------------------------
+
+int ensure_stage(DevicePlan* p, size_t bytes) {
+    if (p->stage_bytes >= bytes) return 0;
+    if (p->d_stage) cudaFree(p->d_stage);
+    p->d_stage = nullptr;
+    p->stage_bytes = 0;
+    cudaError_t e = cudaMalloc(&p->d_stage, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "staging allocation");
+    p->stage_bytes = bytes;
+    return 0;
+}
+
+int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t st);
+
+int execute_request(const faf_transform* t, Request& r) {
+    DevicePlan* p = plan_of(t);
+    if (!p) return fail("transform has no CUDA plan");
+    if (r.batch <= 0) return 0;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != p->device) cudaSetDevice(p->device);
+    const cudaStream_t st = p->stream;
+    const void* ptrs[4] = {r.in_a, r.in_b, r.out_a, r.out_b};
+    int ndev = 0, nptr = 0;
+    for (const void* q : ptrs) {
+        if (!q) continue;
+        nptr++;
+        ndev += ptr_is_device(q);
+    }
+    int rc = 0;
+    if (ndev == nptr) {
+        rc = run_device(t, p, r, st);
+        if (rc == 0 && !p->user_stream) {
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) rc = cuda_fail(e, "execute");
+        }
+    } else if (ndev == 0) {
+        // Host buffers: copy in, run, copy out, synchronise.
+        std::lock_guard<std::mutex> lock(p->mu);
+        const size_t fin = span_floats(r.batch, r.in_dist, r.in_len, r.in_fpe);
+        const size_t fout = span_floats(r.batch, r.out_dist, r.out_len, r.out_fpe);
+        const int nin = r.in_b ? 2 : 1, nout = r.out_b ? 2 : 1;
+        const size_t total = (fin * nin + fout * nout) * sizeof(float) + 256;
+        if ((rc = ensure_stage(p, total)) != 0) goto done;
+        {
+            float* base = (float*)p->d_stage;
+            Request d = r;
+            float* slots[4] = {base, base + fin, base + fin * nin, base + fin * nin + fout};
+            cudaError_t e = cudaSuccess;
+            d.in_a = slots[0];
+            e = cudaMemcpyAsync(slots[0], r.in_a, fin * sizeof(float), cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess && r.in_b) {
+                d.in_b = slots[1];
+                e = cudaMemcpyAsync(slots[1], r.in_b, fin * sizeof(float),
+                                    cudaMemcpyHostToDevice, st);
+            }
+            d.out_a = slots[2];
+            d.out_b = r.out_b ? slots[3] : nullptr;
+            if (e != cudaSuccess) { rc = cuda_fail(e, "host-to-device copy"); goto done; }
+            if ((rc = run_device(t, p, d, st)) != 0) goto done;
+            e = cudaMemcpyAsync(r.out_a, d.out_a, fout * sizeof(float), cudaMemcpyDeviceToHost,
+                                st);
+            if (e == cudaSuccess && r.out_b)
+                e = cudaMemcpyAsync(r.out_b, d.out_b, fout * sizeof(float),
+                                    cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) rc = cuda_fail(e, "device-to-host copy");
+        }
+    } else {
+        rc = fail("execute buffers mix host and device memory");
+    }
+done:
+    if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
+    return rc;
+}
+
+// Pipeline with ops that must run on the host: R2C kernel -> host ops ->
+// C2R kernel, through a device spectrum buffer.
+int pipeline_host_ops(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t st) {
+    const size_t n = t->n, nb = n / 2 + 1;
+    const size_t spec_floats = 2 * nb * (size_t)r.batch;
+    float* d_spec = nullptr;
+    cudaError_t e = cudaMalloc(&d_spec, spec_floats * sizeof(float));
+    if (e != cudaSuccess) return cuda_fail(e, "pipeline spectrum allocation");
+    std::vector<float> h(spec_floats);
+    DevicePlan* fwd = plan_of(t->inner);
+    int rc = 0;
+    e = fafp::exec_r2c(fwd, r.in_a, d_spec, d_spec + nb * r.batch, r.batch,
+                       r.in_dist ? r.in_dist : (long long)n, (long long)nb, false, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h.data(), d_spec, spec_floats * sizeof(float), cudaMemcpyDeviceToHost,
+                            st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) {
+        for (long long b = 0; b < r.batch; b++)
+            apply_ops_host(t, h.data() + b * nb, h.data() + nb * r.batch + b * nb, nb);
+        if (!t->inner_inv) {
+            // analysis pipeline: the spectrum is the output
+            const long long od = r.out_dist ? r.out_dist : (long long)nb;
+            for (long long b = 0; b < r.batch && e == cudaSuccess; b++) {
+                e = cudaMemcpyAsync(r.out_a + b * od, h.data() + b * nb, nb * sizeof(float),
+                                    cudaMemcpyHostToDevice, st);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(r.out_b + b * od, h.data() + nb * r.batch + b * nb,
+                                        nb * sizeof(float), cudaMemcpyHostToDevice, st);
+            }
+        } else {
+            e = cudaMemcpyAsync(d_spec, h.data(), spec_floats * sizeof(float),
+                                cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess)
+                e = fafp::exec_c2r(plan_of(t->inner_inv), d_spec, d_spec + nb * r.batch, r.out_a,
+                                   r.batch, (long long)nb, r.out_dist ? r.out_dist : (long long)n,
+                                   false, st);
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    if (e != cudaSuccess) rc = cuda_fail(e, "pipeline (host ops)");
+    cudaFree(d_spec);
+    note_launches(2);
+    return rc;
+}
+
+int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t st) {
+    cudaError_t e = cudaSuccess;
+    const long long in_dist = r.in_dist ? r.in_dist : (long long)r.in_len;
+    const long long out_dist = r.out_dist ? r.out_dist : (long long)r.out_len;
+    int launches = 1;
+    switch (t->type) {
+    case FAF_TRANSFORM_FFT:
+    case FAF_TRANSFORM_IFFT:
+        e = fafp::exec_c2c(p, r.in_a, r.in_b, r.out_a, r.out_b, r.batch, in_dist, out_dist,
+                           r.interleaved, nullptr, st);
+        break;
+    case FAF_TRANSFORM_RFFT:
+        e = fafp::exec_r2c(p, r.in_a, r.out_a, r.out_b, r.batch, in_dist, out_dist,
+                           r.interleaved, st);
+        break;
+    case FAF_TRANSFORM_IRFFT:
+        e = fafp::exec_c2r(p, r.in_a, r.in_b, r.out_a, r.batch, in_dist, out_dist, r.interleaved,
+                           st);
+        break;
+    case FAF_TRANSFORM_PIPELINE: {
+        fafk::PipeOp ops[fafk::kMaxOps];
+        bool host_ops = false;
+        const int nops = resolve_pipeline_ops(t, ops, fafk::kMaxOps, &host_ops, st);
+        if (nops < 0) return -1;
+        if (host_ops || !t->inner_inv) return pipeline_host_ops(t, p, r, st);
+        e = fafp::exec_pipeline(p, r.in_a, r.out_a, r.batch, in_dist, out_dist, ops, nops, st);
+        break;
+    }
+    case FAF_TRANSFORM_STFT:
+        if (r.framed) {
+            DevicePlan* fp = plan_of(t->inner);
+            const long long sig_dist = r.in_dist ? r.in_dist : r.sig_len;
+            if (r.batch > 1 && sig_dist != r.sig_len)
+                return fail("batched STFT signals must be packed (in_dist = signal length)");
+            if (r.batch > 1 && r.out_dist && r.out_dist != (long long)r.out_len)
+                return fail("batched STFT output must be packed");
+            e = fafp::exec_stft(fp, r.in_a, r.out_a, r.out_b, r.batch, r.sig_len, r.frames,
+                                r.interleaved, st);
+        } else {
+            DevicePlan* fp = plan_of(t->inner);
+            e = fafp::exec_c2c(p, r.in_a, r.in_b, r.out_a, r.out_b, r.batch, in_dist, out_dist,
+                               r.interleaved, fp ? fp->d_window : nullptr, st);
+            if (!fp) return fail("STFT frame window is unavailable for this size");
+        }
+        break;
+    default:
+        return fail("transform type '%s' is not on the CUDA path", faf_transform_name(t->type));
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+    note_launches(launches);
+    return 0;
+}
+
+int build_request(const faf_transform* t, faf_buffer* out, const faf_buffer* in, Request& r) {
+    switch (t->type) {
+    case FAF_TRANSFORM_PIPELINE: return check_pipeline(t, out, in, r);
+    case FAF_TRANSFORM_RFFT:
+    case FAF_TRANSFORM_IRFFT: return check_rfft(t, out, in, r);
+    case FAF_TRANSFORM_STFT: return check_stft(t, out, in, r);
+    case FAF_TRANSFORM_FFT:
+    case FAF_TRANSFORM_IFFT: return check_layouts_c2c(t, out, in, r);
+    default: return fail("transform type '%s' is not on the CUDA path", faf_transform_name(t->type));
+    }
+}
+
+}  // namespace
+
+extern "C" int faf_execute(const faf_transform* t, faf_buffer* out, const faf_buffer* in) {
+    if (!t || !out || !in) return -1;
+    Request r;
+    if (build_request(t, out, in, r) != 0) return -1;
+    return execute_request(t, r);
+}
+
+extern "C" int faf_execute_batched(const faf_transform* t, faf_buffer* out, const faf_buffer* in,
+                                   size_t batch, size_t in_dist, size_t out_dist) {
+    if (!t || !out || !in) return fail("faf_execute_batched: NULL argument");
+    Request r;
+    if (build_request(t, out, in, r) != 0) return -1;
+    r.batch = (long long)batch;
+    r.in_dist = (long long)in_dist;
+    r.out_dist = (long long)out_dist;
+    if (in_dist && in_dist < r.in_len) return fail("in_dist %zu < transform input length %zu", in_dist, r.in_len);
+    if (out_dist && out_dist < r.out_len) return fail("out_dist %zu < transform output length %zu", out_dist, r.out_len);
+    return execute_request(t, r);
+}
+
+namespace fafapi {
+
+int exec_split_one(const faf_transform* t, void* out_re, void* out_im, const void* in_re,
+                   const void* in_im) {
+    if (!t) return -1;
+    faf_buffer in = faf_buffer_split((void*)in_re, (void*)in_im, t->n);
+    faf_buffer out = faf_buffer_split(out_re, out_im, t->n);
+    Request r;
+    faf_transform tmp = *t;
+    tmp.cfg.layout = FAF_LAYOUT_SPLIT;
+    if (check_layouts_c2c(&tmp, &out, &in, r) != 0) return -1;
+    return execute_request(t, r);
+}
+
+}  // namespace fafapi
+
+// ---- streams --------------------------------------------------------------
+
+extern "C" int faf_cuda_set_stream(faf_transform* t, void* stream) {
+    DevicePlan* p = plan_of(t);
+    if (!p) return fail("faf_cuda_set_stream: transform has no CUDA plan");
+    p->stream = (cudaStream_t)stream;
+    p->user_stream = stream != nullptr;
+    // nested plans follow the outer transform
+    if (t->inner) faf_cuda_set_stream(t->inner, stream);
+    if (t->inner_inv) faf_cuda_set_stream(t->inner_inv, stream);
+    return 0;
+}
+
+extern "C" void* faf_cuda_get_stream(const faf_transform* t) {
+    DevicePlan* p = plan_of(t);
+    return p ? (void*)p->stream : nullptr;
+}
+
+extern "C" int faf_cuda_synchronize(const faf_transform* t) {
+    DevicePlan* p = plan_of(t);
+    if (!p) return fail("faf_cuda_synchronize: transform has no CUDA plan");
+    cudaError_t e = cudaStreamSynchronize(p->stream);
+    return e == cudaSuccess ? 0 : cuda_fail(e, "synchronize");
+}
+
+extern "C" int faf_cuda_available(void) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        fail("no CUDA device: %s", e == cudaSuccess ? "count is 0" : cudaGetErrorString(e));
+        return 0;
+    }
+    return 1;
+}
+
+extern "C" const char* faf_cuda_plan_kind(const faf_transform* t) {
+    DevicePlan* p = plan_of(t);
+    if (!p) return nullptr;
+    switch (p->kind) {
+    case Kind::C2C: return "c2c";
+    case Kind::C2C_LARGE: return "c2c-4step";
+    case Kind::RADER: return "rader";
+    case Kind::BLUESTEIN: return "bluestein";
+    case Kind::R2C: return "r2c";
+    case Kind::C2R: return "c2r";
+    case Kind::PIPELINE: return "pipeline";
+    case Kind::STFT: return "stft";
+    }
+    return "unknown";
+}
+

@@ -1,0 +1,97 @@
+// faf_kernels.cuh -- kernel argument blocks and host launchers shared by the
+// planner (faf_plan.cu) and the kernels (faf_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "faf_types.h"
+
+namespace fafk {
+
+// Launch geometry chosen by the planner for one Shape.
+struct Geometry {
+    int E;          // values per thread per stage (16 or 32)
+    int G;          // transforms per CTA
+    int threads;    // G * T
+    size_t smem;    // dynamic shared memory bytes
+};
+
+// Spectral op codes used inside the fused pipeline kernel.
+enum : int { OP_NONE = 0, OP_CONJ = 1, OP_MUL = 2, OP_BANDPASS = 3 };
+constexpr int kMaxOps = 8;
+
+struct PipeOp {
+    int code;
+    int lo, hi;          // BANDPASS bins kept: [lo, hi]
+    int m;               // MUL: bins used = min(bound bins, n/2+1)
+    const float* hr;     // MUL: device H planes
+    const float* hi_;
+};
+
+struct C2CArgs {
+    const float* in_re;
+    const float* in_im;   // NULL for interleaved
+    float* out_re;
+    float* out_im;        // NULL for interleaved
+    long long in_dist, out_dist;  // floats between transforms (per plane)
+    long long batch;
+    float scale;
+    float sgn;            // +1 forward, -1 inverse (conjugation trick)
+    int interleaved;
+    const float* window;  // optional per-sample real window (STFT frame), or NULL
+};
+
+struct RealArgs {  // R2C / C2R / pipeline / STFT
+    const float* in_a;    // R2C: x; C2R: X re
+    const float* in_b;    // C2R: X im
+    float* out_a;         // R2C: X re; C2R / pipeline: y
+    float* out_b;         // R2C: X im
+    long long in_dist, out_dist;
+    long long batch;
+    float scale;
+    int interleaved;      // Hermitian side is interleaved (re,im) pairs
+    const float2* stw;    // super-twiddles exp(-i*pi*((k+1)/nc + 1/2)), k < nc/2
+    // STFT framing
+    const float* window;
+    int win, hop;
+    long long sig_len, frames;
+    // pipeline
+    int nops;
+    PipeOp ops[kMaxOps];
+};
+
+struct ConvArgs {  // Rader (prime n) and Bluestein (any n)
+    const float* in_re;
+    const float* in_im;
+    float* out_re;
+    float* out_im;
+    long long in_dist, out_dist;
+    long long batch;
+    float scale;
+    float sgn;
+    int n;                 // outer length
+    const int* rin;        // Rader gather  x[rin[j]]
+    const int* rout;       // Rader scatter y[rout[j]]
+    const float2* phi;     // Bluestein chirp, n entries
+    const float2* B;       // FFT of the convolution kernel, inner length
+    float inv_inner;       // 1 / inner length
+};
+
+// Host launchers (return a cudaError_t).  `S` is the inner FFT shape.
+cudaError_t launch_c2c(const fafd::Shape& S, const Geometry& g, const float2* tw,
+                       const C2CArgs& a, cudaStream_t st);
+cudaError_t launch_r2c(const fafd::Shape& S, const Geometry& g, const float2* tw,
+                       const RealArgs& a, cudaStream_t st);
+cudaError_t launch_c2r(const fafd::Shape& S, const Geometry& g, const float2* tw,
+                       const RealArgs& a, cudaStream_t st);
+cudaError_t launch_pipeline(const fafd::Shape& S, const Geometry& g, const float2* tw,
+                            const RealArgs& a, cudaStream_t st);
+cudaError_t launch_stft(const fafd::Shape& S, const Geometry& g, const float2* tw,
+                        const RealArgs& a, cudaStream_t st);
+cudaError_t launch_rader(const fafd::Shape& S, const Geometry& g, const float2* tw,
+                         const ConvArgs& a, cudaStream_t st);
+cudaError_t launch_bluestein(const fafd::Shape& S, const Geometry& g, const float2* tw,
+                             const ConvArgs& a, cudaStream_t st);
+
+}  // namespace fafk

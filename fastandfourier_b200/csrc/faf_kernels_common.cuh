@@ -1,0 +1,235 @@
+// faf_kernels_common.cuh -- sources, sinks and helpers of the batched
+// transform kernels for sm_100a (one .cu per kernel family includes this).
+//
+// Every kernel runs G transforms per CTA (T threads each) through the
+// Stockham engine of faf_device.cuh.  Loads of the first stage and stores of
+// the last stage go straight between global memory and registers, so a
+// plain C2C reads its input once and writes its output once; everything the
+// reference does as separate passes over the data (R2C pack / super-twiddle
+// post-pass, the pipeline's spectral ops, the C2R pre-pass, STFT windowing,
+// Rader gather / scatter, Bluestein chirp multiplies, the norm scaling) is
+// fused into the sources / sinks of those stages.
+#pragma once
+
+#include "faf_device.cuh"
+#include "faf_kernels.cuh"
+
+namespace fafk {
+// Values held per thread per stage.  With 16, a transform of n points uses
+// about n/16 threads, so the single-CTA kernels cover n <= 16384 (radix-16
+// stages) within the 1024-thread limit; larger n use the four-step path.
+constexpr int kE = 16;
+using fafd::cf;
+using fafd::run_fft;
+using fafd::Shape;
+using fafd::SmemConjSrc;
+using fafd::SmemIO;
+
+// ---------------------------------------------------------------------------
+// Sources and sinks
+// ---------------------------------------------------------------------------
+
+struct SplitSrc {  // split or interleaved complex input, optional real window
+    const float* re;
+    const float* im;
+    const float* win;
+    float sgn;
+    int inter;
+    bool live;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ cf get(int i) const {
+        if (!live) return cf{0.f, 0.f};
+        float r, m;
+        if (inter) {
+            float2 v = __ldcs(reinterpret_cast<const float2*>(re) + i);
+            r = v.x; m = v.y;
+        } else {
+            r = __ldcs(re + i); m = __ldcs(im + i);
+        }
+        if (win) { float w = __ldg(win + i); r *= w; m *= w; }
+        return cf{r, sgn * m};
+    }
+};
+
+struct SplitSink {
+    float* re;
+    float* im;
+    float scale;
+    float sgn;
+    int inter;
+    bool live;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ void put(int i, cf v) const {
+        if (!live) return;
+        if (inter) {
+            __stcs(reinterpret_cast<float2*>(re) + i, make_float2(v.x * scale, sgn * v.y * scale));
+        } else {
+            __stcs(re + i, v.x * scale);
+            __stcs(im + i, sgn * v.y * scale);
+        }
+    }
+};
+
+// z[k] = x[2k] + i x[2k+1] (R2C packing, reference src/faf_rfft.c:356-359).
+struct RealPairSrc {
+    const float* x;
+    bool live;
+    bool vec;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ cf get(int i) const {
+        if (!live) return cf{0.f, 0.f};
+        if (vec) {
+            float2 v = __ldcs(reinterpret_cast<const float2*>(x) + i);
+            return cf{v.x, v.y};
+        }
+        return cf{__ldcs(x + 2 * i), __ldcs(x + 2 * i + 1)};
+    }
+};
+
+// Windowed, zero-padded STFT frame packed as real pairs.
+struct FrameSrc {
+    const float* x;   // frame start
+    const float* w;
+    int win;
+    bool live;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ cf get(int i) const {
+        const int a = 2 * i, b = a + 1;
+        float v0 = 0.f, v1 = 0.f;
+        if (live && a < win) v0 = __ldg(x + a) * __ldg(w + a);
+        if (live && b < win) v1 = __ldg(x + b) * __ldg(w + b);
+        return cf{v0, v1};
+    }
+};
+
+// y[2k] = Re z, y[2k+1] = Im z, with the conjugation of an inverse FFT undone
+// (C2R unpack, reference src/faf_rfft.c:392-395).
+struct RealPairSink {
+    float* y;
+    float scale;
+    bool live;
+    bool vec;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ void put(int i, cf v) const {
+        if (!live) return;
+        if (vec) {
+            __stcs(reinterpret_cast<float2*>(y) + i, make_float2(v.x * scale, -v.y * scale));
+        } else {
+            __stcs(y + 2 * i, v.x * scale);
+            __stcs(y + 2 * i + 1, -v.y * scale);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Launch helpers
+// ---------------------------------------------------------------------------
+
+template <class K>
+inline cudaError_t prep(K kernel, size_t smem) {
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+inline unsigned grid_for(long long batch, int G) {
+    return (unsigned)((batch + G - 1) / G);
+}
+
+// Per-CTA group bookkeeping: transform group g, thread t within it, planes.
+struct Group {
+    int g, t;
+    float* re;
+    float* im;
+};
+
+__device__ __forceinline__ Group group_of(const Shape& S, float* sm, int extra_per_group) {
+    Group q;
+    q.g = threadIdx.x / S.T;
+    q.t = threadIdx.x - q.g * S.T;
+    q.re = sm + (size_t)q.g * (2 * S.plane + extra_per_group);
+    q.im = q.re + S.plane;
+    return q;
+}
+
+// ---------------------------------------------------------------------------
+// R2C: pack -> nc-point FFT -> super-twiddle post-pass (src/faf_rfft.c:61-89)
+// ---------------------------------------------------------------------------
+
+// Post-pass of one bin pair (k, nc-k), k >= 1, from the packed spectrum Z.
+__device__ __forceinline__ void r2c_pair(cf zk, cf znk, float2 w, cf& Xk, cf& Xnk) {
+    // f1 = Z[k] + conj(Z[nc-k]), f2 = Z[k] - conj(Z[nc-k]), t = f2 * w
+    const float f1r = zk.x + znk.x, f1i = zk.y - znk.y;
+    const float f2r = zk.x - znk.x, f2i = zk.y + znk.y;
+    const float tr = f2r * w.x - f2i * w.y, ti = fmaf(f2r, w.y, f2i * w.x);
+    Xk = cf{0.5f * (f1r + tr), 0.5f * (f1i + ti)};
+    Xnk = cf{0.5f * (f1r - tr), 0.5f * (ti - f1i)};
+}
+
+// Pre-pass of one bin pair for the C2R (src/faf_rfft.c:122-146); w is the
+// forward super-twiddle, the inverse uses its conjugate.
+__device__ __forceinline__ void c2r_pair(cf xk, cf xnk, float2 w, cf& Zk, cf& Znk) {
+    const float fer = xk.x + xnk.x, fei = xk.y - xnk.y;  // fk + conj(X[nc-k])
+    const float dr = xk.x - xnk.x, di = xk.y + xnk.y;    // fk - conj(X[nc-k])
+    const float wr = w.x, wi = -w.y;
+    const float orr = dr * wr - di * wi, oi = fmaf(dr, wi, di * wr);
+    Zk = cf{fer + orr, fei + oi};
+    Znk = cf{fer - orr, -(fei - oi)};
+}
+
+struct HermSink {  // split or interleaved Hermitian output
+    float* re;
+    float* im;
+    int inter;
+    __device__ __forceinline__ void put(int k, float r, float i) const {
+        if (inter) {
+            __stcs(reinterpret_cast<float2*>(re) + k, make_float2(r, i));
+        } else {
+            __stcs(re + k, r);
+            __stcs(im + k, i);
+        }
+    }
+};
+
+template <int E, class Src>
+__device__ __forceinline__ void r2c_body(const Shape& S, const Group& q,
+                                         const float2* __restrict__ tw,
+                                         const float2* __restrict__ stw, const Src& src,
+                                         const HermSink& out, float scale, bool live) {
+    const int nc = S.n;
+    const SmemIO mid{q.re, q.im};
+    run_fft<E>(S, q.t, q.re, q.im, tw, src, mid);
+    __syncthreads();
+    if (!live) return;
+    for (int k = q.t; k <= nc / 2; k += S.T) {
+        if (k == 0) {
+            const cf z = mid.get(0);
+            out.put(0, (z.x + z.y) * scale, 0.f);
+            out.put(nc, (z.x - z.y) * scale, 0.f);
+        } else {
+            cf Xk, Xnk;
+            r2c_pair(mid.get(k), mid.get(nc - k), __ldg(&stw[k - 1]), Xk, Xnk);
+            if (k != nc - k) out.put(k, Xk.x * scale, Xk.y * scale);
+            out.put(nc - k, Xnk.x * scale, Xnk.y * scale);
+        }
+    }
+}
+
+#define FAF_REAL_LAUNCH(NAME, KERNEL, ...)                                                     \
+    cudaError_t NAME(const Shape& S, const Geometry& g, const float2* tw, const RealArgs& a,  \
+                     cudaStream_t st) {                                                        \
+        if (a.batch <= 0) return cudaSuccess;                                                  \
+        cudaError_t e;                                                                         \
+        if ((e = prep(KERNEL<kE>, g.smem)) != cudaSuccess) return e;                           \
+        KERNEL<kE><<<grid_for(a.batch, g.G), g.threads, g.smem, st>>>(S, tw, a, g.G __VA_ARGS__); \
+        return cudaGetLastError();                                                             \
+    }
+
+inline bool vec_ok(const void* p, long long dist) {
+    return (((unsigned long long)(size_t)p) % 8 == 0) && (dist % 2 == 0);
+}
+
+}  // namespace fafk

@@ -1,0 +1,481 @@
+// faf_plan.cu -- planner: radix programs, FP64 tables, launch geometry and
+// device-pointer execution for every plan kind.
+#include "faf_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace fafp {
+
+namespace {
+
+constexpr int kE = 16;                        // values per thread per stage
+constexpr size_t kMaxSmem = 227 * 1024;       // dynamic shared memory per CTA
+constexpr int kTargetThreads = 256;
+
+template <class T>
+cudaError_t upload(T** dst, const T* src, size_t count) {
+    *dst = nullptr;
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void**)dst, count * sizeof(T));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+bool cuda_ok(cudaError_t e, std::string& err, const char* what) {
+    if (e == cudaSuccess) return true;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+}
+
+unsigned long long powmod(unsigned long long b, unsigned long long e, unsigned long long m) {
+    unsigned long long r = 1;
+    b %= m;
+    while (e) {
+        if (e & 1) r = r * b % m;
+        b = b * b % m;
+        e >>= 1;
+    }
+    return r;
+}
+
+int primitive_root(int p) {
+    const int phi = p - 1;
+    std::vector<int> pf;
+    int m = phi;
+    for (int d = 2; (long long)d * d <= m; d++)
+        if (m % d == 0) {
+            pf.push_back(d);
+            while (m % d == 0) m /= d;
+        }
+    if (m > 1) pf.push_back(m);
+    for (int g = 2; g < p; g++) {
+        bool ok = true;
+        for (int q : pf)
+            if (powmod(g, phi / q, p) == 1) { ok = false; break; }
+        if (ok) return g;
+    }
+    return 0;
+}
+
+bool is_5_smooth(long long n) {
+    if (n <= 0) return false;
+    for (int p : {2, 3, 5}) while (n % p == 0) n /= p;
+    return n == 1;
+}
+
+long long next_5_smooth(long long m) {
+    if (m <= 1) return 1;
+    while (!is_5_smooth(m)) m++;
+    return m;
+}
+
+// FP64 twiddles W_n^i = exp(-2 pi i i / n).
+std::vector<float2> twiddles(int n) {
+    std::vector<float2> w(std::max(n, 1));
+    for (int i = 0; i < n; i++) {
+        const double a = -2.0 * M_PI * (double)i / (double)n;
+        w[i] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    return w;
+}
+
+void fft_rec(const double* xr, const double* xi, int n, int stride, double* yr, double* yi) {
+    if (n == 1) {
+        yr[0] = xr[0];
+        yi[0] = xi[0];
+        return;
+    }
+    int p = 2;
+    while (n % p) p++;
+    const int m = n / p;
+    std::vector<double> tr(n), ti(n);
+    for (int r = 0; r < p; r++)
+        fft_rec(xr + (size_t)r * stride, xi + (size_t)r * stride, m, stride * p, &tr[r * m],
+                &ti[r * m]);
+    for (int k = 0; k < n; k++) {
+        double sr = 0, si = 0;
+        for (int r = 0; r < p; r++) {
+            const long long e = ((long long)r * k) % n;
+            const double a = -2.0 * M_PI * (double)e / (double)n;
+            const double c = std::cos(a), s = std::sin(a);
+            const double ur = tr[r * m + k % m], ui = ti[r * m + k % m];
+            sr += ur * c - ui * s;
+            si += ur * s + ui * c;
+        }
+        yr[k] = sr;
+        yi[k] = si;
+    }
+}
+
+}  // namespace
+
+void host_dft_fp64(std::vector<double>& re, std::vector<double>& im) {
+    const int n = (int)re.size();
+    std::vector<double> yr(n), yi(n);
+    fft_rec(re.data(), im.data(), n, 1, yr.data(), yi.data());
+    re.swap(yr);
+    im.swap(yi);
+}
+
+// Radix program: 16s first, then one 8/4/2 for the rest of the power of two,
+// then 5s, 3s and 7s.  Any stage order is a valid Stockham program; large
+// radices first keeps the number of shared-memory passes minimal.
+bool radix_program(int n, std::vector<int>& r) {
+    r.clear();
+    if (n < 1) return false;
+    int m = n, c2 = 0;
+    while (m % 2 == 0) { m /= 2; c2++; }
+    while (c2 >= 4) { r.push_back(16); c2 -= 4; }
+    if (c2 == 3) r.push_back(8);
+    if (c2 == 2) r.push_back(4);
+    if (c2 == 1) r.push_back(2);
+    while (m % 5 == 0) { r.push_back(5); m /= 5; }
+    while (m % 3 == 0) { r.push_back(3); m /= 3; }
+    while (m % 7 == 0) { r.push_back(7); m /= 7; }
+    return m == 1;
+}
+
+fafd::Shape FftSize::shape(int slots) const {
+    fafd::Shape s;
+    s.n = n;
+    s.ns = (int)stages.size();
+    s.T = T;
+    s.plane = plane_floats(slots);
+    s.st = d_stages;
+    return s;
+}
+
+int plane_floats(int slots) {
+    const int last = std::max(slots, 1) - 1;
+    int p = last + (last >> 5) + 1;
+    return (p + 1) & ~1;
+}
+
+bool build_size(int n, FftSize& out, std::string& err) {
+    out = FftSize();
+    out.n = n;
+    std::vector<int> rad;
+    if (!radix_program(n, rad)) {
+        err = "size " + std::to_string(n) + " is not 7-smooth";
+        return false;
+    }
+    int T = 1, p = 1;
+    for (int R : rad) {
+        const int mb = std::max(1, kE / R);
+        const int need = ((n / R) + mb - 1) / mb;
+        T = std::max(T, need);
+        out.stages.push_back(fafd::Stage{R, p, n / (p * R), 0});
+        p *= R;
+    }
+    if (T > 1024) {
+        err = "size " + std::to_string(n) + " exceeds one CTA";
+        return false;
+    }
+    out.T = T;
+    std::vector<float2> w = twiddles(n);
+    if (!cuda_ok(upload(&out.d_tw, w.data(), w.size()), err, "twiddle upload")) return false;
+    if (!out.stages.empty() &&
+        !cuda_ok(upload(&out.d_stages, out.stages.data(), out.stages.size()), err,
+                 "stage upload"))
+        return false;
+    if (out.stages.empty()) {
+        // n == 1: keep a valid pointer for the kernels.
+        fafd::Stage dummy{1, 1, 1, 0};
+        if (!cuda_ok(upload(&out.d_stages, &dummy, 1), err, "stage upload")) return false;
+    }
+    return true;
+}
+
+void free_size(FftSize& s) {
+    cudaFree(s.d_stages);
+    cudaFree(s.d_tw);
+    s.d_stages = nullptr;
+    s.d_tw = nullptr;
+}
+
+fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long batch) {
+    fafk::Geometry g;
+    g.E = kE;
+    const size_t per = (size_t)(2 * plane_floats(slots) + extra_floats) * sizeof(float);
+    int G = std::max(1, kTargetThreads / s.T);
+    G = std::min<long long>(G, std::max(1LL, batch));
+    while (G > 1 && ((size_t)G * per > kMaxSmem || G * s.T > 1024)) G--;
+    g.G = G;
+    g.threads = G * s.T;
+    g.smem = (size_t)G * per;
+    return g;
+}
+
+// ---------------------------------------------------------------------------
+// Plan creation
+// ---------------------------------------------------------------------------
+
+static DevicePlan* new_plan(Kind k, int n) {
+    DevicePlan* p = new DevicePlan();
+    p->kind = k;
+    p->n = n;
+    cudaGetDevice(&p->device);
+    return p;
+}
+
+void plan_free(DevicePlan* p) {
+    if (!p) return;
+    free_size(p->inner);
+    free_size(p->f1);
+    free_size(p->f2);
+    cudaFree(p->d_tw_big);
+    cudaFree(p->d_stw);
+    cudaFree(p->d_B);
+    cudaFree(p->d_phi);
+    cudaFree(p->d_rin);
+    cudaFree(p->d_rout);
+    cudaFree(p->d_window);
+    cudaFree(p->d_stage);
+    cudaFree(p->d_scratch);
+    delete p;
+}
+
+static bool is_prime(int n) {
+    if (n < 2) return false;
+    for (int d = 2; (long long)d * d <= n; d++)
+        if (n % d == 0) return false;
+    return true;
+}
+
+static bool is_7_smooth(long long n) {
+    if (n <= 0) return false;
+    for (int p : {2, 3, 5, 7}) while (n % p == 0) n /= p;
+    return n == 1;
+}
+
+DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::string& err) {
+    (void)flags;
+    DevicePlan* p = nullptr;
+    if (is_7_smooth(n)) {
+        if (n > kMaxSingleCta) {
+            err = "C2C length " + std::to_string(n) + " needs the four-step path";
+            return nullptr;
+        }
+        p = new_plan(Kind::C2C, n);
+        if (!build_size(n, p->inner, err)) { plan_free(p); return nullptr; }
+    } else if (is_prime(n) && is_7_smooth(n - 1)) {
+        // Rader: y = x0 + IDFT_m(DFT_m(x[g^j]) * DFT_m(W_p^{g^-j}))[...]
+        const int m = n - 1;
+        if (m > kMaxSingleCta) {
+            err = "Rader prime " + std::to_string(n) + " exceeds the single-CTA inner length";
+            return nullptr;
+        }
+        p = new_plan(Kind::RADER, n);
+        if (!build_size(m, p->inner, err)) { plan_free(p); return nullptr; }
+        const int g = primitive_root(n);
+        const int ginv = (int)powmod(g, n - 2, n);
+        std::vector<int> rin(m), rout(m);
+        std::vector<double> br(m), bi(m);
+        long long a = 1, b = 1;
+        for (int j = 0; j < m; j++) {
+            rin[j] = (int)a;
+            rout[j] = (int)b;
+            a = a * g % n;
+            b = b * ginv % n;
+        }
+        for (int j = 0; j < m; j++) {
+            const double ang = -2.0 * M_PI * (double)rout[j] / (double)n;
+            br[j] = std::cos(ang);
+            bi[j] = std::sin(ang);
+        }
+        host_dft_fp64(br, bi);
+        std::vector<float2> B(m);
+        for (int j = 0; j < m; j++) B[j] = make_float2((float)br[j], (float)bi[j]);
+        if (!cuda_ok(upload(&p->d_rin, rin.data(), m), err, "rader tables") ||
+            !cuda_ok(upload(&p->d_rout, rout.data(), m), err, "rader tables") ||
+            !cuda_ok(upload(&p->d_B, B.data(), m), err, "rader tables")) {
+            plan_free(p);
+            return nullptr;
+        }
+    } else {
+        // Bluestein with M = next 5-smooth >= 2n - 1 (reference
+        // src/faf_bluestein.c:19-22), chirp phi[k] = exp(-i pi k^2 / n).
+        const long long M = next_5_smooth(2LL * n - 1);
+        if (M > kMaxSingleCta) {
+            err = "Bluestein length " + std::to_string(n) + " (M = " + std::to_string(M) +
+                  ") exceeds the single-CTA inner length";
+            return nullptr;
+        }
+        p = new_plan(Kind::BLUESTEIN, n);
+        if (!build_size((int)M, p->inner, err)) { plan_free(p); return nullptr; }
+        std::vector<float2> phi(n);
+        std::vector<double> br(M, 0.0), bi(M, 0.0);
+        for (int k = 0; k < n; k++) {
+            const long long q = ((long long)k * k) % (2LL * n);
+            const double ang = -M_PI * (double)q / (double)n;
+            phi[k] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+            if (k == 0) {
+                br[0] = 1.0;
+            } else {
+                // b[l] = b[M - l] = conj(phi[l])
+                br[k] = std::cos(ang);
+                bi[k] = -std::sin(ang);
+                br[M - k] = br[k];
+                bi[M - k] = bi[k];
+            }
+        }
+        host_dft_fp64(br, bi);
+        std::vector<float2> B(M);
+        for (long long j = 0; j < M; j++) B[j] = make_float2((float)br[j], (float)bi[j]);
+        if (!cuda_ok(upload(&p->d_phi, phi.data(), n), err, "bluestein tables") ||
+            !cuda_ok(upload(&p->d_B, B.data(), (size_t)M), err, "bluestein tables")) {
+            plan_free(p);
+            return nullptr;
+        }
+    }
+    p->inverse = inverse;
+    p->scale = scale;
+    return p;
+}
+
+static bool upload_super_twiddles(DevicePlan* p, int nc, std::string& err) {
+    std::vector<float2> stw(std::max(1, nc / 2));
+    for (int k = 0; k < nc / 2; k++) {
+        const double ph = -M_PI * (((double)(k + 1) / (double)nc) + 0.5);
+        stw[k] = make_float2((float)std::cos(ph), (float)std::sin(ph));
+    }
+    return cuda_ok(upload(&p->d_stw, stw.data(), stw.size()), err, "super-twiddle upload");
+}
+
+DevicePlan* plan_r2c(int n, bool inverse, float scale, std::string& err) {
+    const int nc = n / 2;
+    if (nc > kMaxSingleCta) {
+        err = "real length " + std::to_string(n) + " needs the four-step path";
+        return nullptr;
+    }
+    DevicePlan* p = new_plan(inverse ? Kind::C2R : Kind::R2C, n);
+    p->inverse = inverse;
+    p->scale = scale;
+    if (!build_size(nc, p->inner, err) || !upload_super_twiddles(p, nc, err)) {
+        plan_free(p);
+        return nullptr;
+    }
+    return p;
+}
+
+DevicePlan* plan_pipeline(int n, float scale_fwd, float scale_inv, std::string& err) {
+    DevicePlan* p = plan_r2c(n, false, scale_fwd, err);
+    if (!p) return nullptr;
+    p->kind = Kind::PIPELINE;
+    p->scale2 = scale_inv;
+    return p;
+}
+
+DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err) {
+    DevicePlan* p = plan_r2c(n, false, scale, err);
+    if (!p) return nullptr;
+    p->kind = Kind::STFT;
+    p->win = win;
+    p->hop = hop;
+    // Symmetric Hann, reference src/faf_twiddles.c:159-163.
+    std::vector<float> w(std::max(win, 1));
+    for (int i = 0; i < win; i++)
+        w[i] = win > 1 ? (float)(0.5 * (1.0 - std::cos(2.0 * M_PI * (double)i / (double)(win - 1))))
+                       : 1.0f;
+    if (!cuda_ok(upload(&p->d_window, w.data(), w.size()), err, "window upload")) {
+        plan_free(p);
+        return nullptr;
+    }
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// Device-pointer execution
+// ---------------------------------------------------------------------------
+
+cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, float* out_re,
+                     float* out_im, long long batch, long long in_dist, long long out_dist,
+                     bool interleaved, const float* window, cudaStream_t st) {
+    const float sgn = p->inverse ? -1.0f : 1.0f;
+    if (p->kind == Kind::C2C) {
+        fafk::C2CArgs a;
+        a.in_re = in_re; a.in_im = in_im; a.out_re = out_re; a.out_im = out_im;
+        a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
+        a.scale = p->scale; a.sgn = sgn; a.interleaved = interleaved ? 1 : 0;
+        a.window = window;
+        const int slots = p->inner.n;
+        return fafk::launch_c2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
+                                p->inner.d_tw, a, st);
+    }
+    if (interleaved) return cudaErrorNotSupported;
+    fafk::ConvArgs a;
+    a.in_re = in_re; a.in_im = in_im; a.out_re = out_re; a.out_im = out_im;
+    a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
+    a.scale = p->scale; a.sgn = sgn; a.n = p->n;
+    a.rin = p->d_rin; a.rout = p->d_rout; a.phi = p->d_phi; a.B = p->d_B;
+    a.inv_inner = (float)(1.0 / (double)p->inner.n);
+    const int slots = p->inner.n;
+    if (p->kind == Kind::RADER)
+        return fafk::launch_rader(p->inner.shape(slots), geometry(p->inner, slots, 2, batch),
+                                  p->inner.d_tw, a, st);
+    if (p->kind == Kind::BLUESTEIN)
+        return fafk::launch_bluestein(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
+                                      p->inner.d_tw, a, st);
+    return cudaErrorInvalidValue;
+}
+
+static fafk::RealArgs real_args(DevicePlan* p, long long batch) {
+    fafk::RealArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.batch = batch;
+    a.scale = p->scale;
+    a.stw = p->d_stw;
+    return a;
+}
+
+cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long long batch,
+                     long long in_dist, long long out_dist, bool interleaved, cudaStream_t st) {
+    fafk::RealArgs a = real_args(p, batch);
+    a.in_a = x; a.out_a = Xr; a.out_b = Xi;
+    a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
+    const int slots = p->inner.n + 1;
+    return fafk::launch_r2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
+                            p->inner.d_tw, a, st);
+}
+
+cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, long long batch,
+                     long long in_dist, long long out_dist, bool interleaved, cudaStream_t st) {
+    fafk::RealArgs a = real_args(p, batch);
+    a.in_a = Xr; a.in_b = Xi; a.out_a = y;
+    a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
+    const int slots = p->inner.n + 1;
+    return fafk::launch_c2r(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
+                            p->inner.d_tw, a, st);
+}
+
+cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long batch,
+                          long long in_dist, long long out_dist, const fafk::PipeOp* ops,
+                          int nops, cudaStream_t st) {
+    fafk::RealArgs a = real_args(p, batch);
+    a.in_a = x; a.out_a = y;
+    a.in_dist = in_dist; a.out_dist = out_dist;
+    a.scale = p->scale * p->scale2;  // ops are linear: both norms fold into the store
+    a.nops = std::min(nops, fafk::kMaxOps);
+    for (int i = 0; i < a.nops; i++) a.ops[i] = ops[i];
+    const int slots = p->inner.n + 1;
+    return fafk::launch_pipeline(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
+                                 p->inner.d_tw, a, st);
+}
+
+cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long long n_sig,
+                      long long sig_len, long long frames, bool interleaved, cudaStream_t st) {
+    const long long batch = n_sig * frames;
+    fafk::RealArgs a = real_args(p, batch);
+    a.in_a = x; a.out_a = Xr; a.out_b = Xi;
+    a.out_dist = p->n / 2 + 1;
+    a.interleaved = interleaved;
+    a.window = p->d_window; a.win = p->win; a.hop = p->hop;
+    a.sig_len = sig_len; a.frames = frames;
+    const int slots = p->inner.n + 1;
+    return fafk::launch_stft(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
+                             p->inner.d_tw, a, st);
+}
+
+}  // namespace fafp

@@ -1,0 +1,107 @@
+// faf_plan.h -- host-side planner and device plans for the B200 path.
+//
+// A DevicePlan is what faf_transform.device_plan points to.  It owns every
+// device table of the transform (stage lists, FP64-generated twiddles,
+// super-twiddles, Rader permutations and kernel spectrum, Bluestein chirp,
+// STFT window) and the staging buffers used when a caller passes host
+// memory.  Plans are immutable after creation except for the stream, the
+// lazily grown staging buffers (guarded by `mu`) and the four-step scratch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "faf_kernels.cuh"
+
+namespace fafp {
+
+// Largest transform one CTA holds (radix-16 stages, 16 values per thread,
+// 1024 threads).  Longer transforms take the four-step path.
+constexpr int kMaxSingleCta = 16384;
+constexpr int kMaxLength = 65536;  // the reference's register-file cap (faf.h:95-98)
+
+// One inner FFT size: radix program + device tables.
+struct FftSize {
+    int n = 0;
+    int T = 1;
+    std::vector<fafd::Stage> stages;
+    fafd::Stage* d_stages = nullptr;
+    float2* d_tw = nullptr;   // W_n^i, i < n (forward), from FP64
+    fafd::Shape shape(int slots) const;
+};
+
+bool radix_program(int n, std::vector<int>& radices);
+bool build_size(int n, FftSize& out, std::string& err);
+void free_size(FftSize& s);
+int plane_floats(int slots);
+fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long batch);
+
+enum class Kind {
+    C2C,        // single-CTA C2C (5-smooth / codelet / 7-smooth inner sizes)
+    C2C_LARGE,  // four-step C2C through per-CTA scratch (n > kMaxSingleCta)
+    RADER,      // prime n, fused gather / FFT_{n-1} / x B / IFFT / scatter
+    BLUESTEIN,  // any n, fused chirp / FFT_M / x B / IFFT_M / chirp
+    R2C,
+    C2R,
+    PIPELINE,   // fused R2C -> ops -> C2R
+    STFT        // framed, windowed R2C
+};
+
+struct DevicePlan {
+    Kind kind = Kind::C2C;
+    int device = 0;
+    int n = 0;             // outer length (real length for R2C family)
+    bool inverse = false;  // C2C direction (conjugation trick)
+    float scale = 1.0f;    // norm scale of this transform
+    float scale2 = 1.0f;   // pipeline: inverse-side scale
+    FftSize inner;         // the FFT the kernels run
+    // four-step factors (C2C_LARGE)
+    FftSize f1, f2;
+    int n1 = 0, n2 = 0;
+    float2* d_tw_big = nullptr;  // W_n^i for the four-step middle twiddles
+    // tables
+    float2* d_stw = nullptr;     // R2C super-twiddles
+    float2* d_B = nullptr;       // Rader / Bluestein kernel spectrum
+    float2* d_phi = nullptr;     // Bluestein chirp
+    int* d_rin = nullptr;        // Rader gather
+    int* d_rout = nullptr;       // Rader scatter
+    float* d_window = nullptr;   // STFT window
+    int win = 0, hop = 0;
+    // launch state
+    cudaStream_t stream = nullptr;  // 0 = legacy default stream
+    bool user_stream = false;
+    // staging for host buffers and four-step scratch
+    std::mutex mu;
+    void* d_stage = nullptr;
+    size_t stage_bytes = 0;
+    void* d_scratch = nullptr;
+    size_t scratch_bytes = 0;
+};
+
+DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::string& err);
+DevicePlan* plan_r2c(int n, bool inverse, float scale, std::string& err);
+DevicePlan* plan_pipeline(int n, float scale_fwd, float scale_inv, std::string& err);
+DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err);
+void plan_free(DevicePlan* p);
+
+// Device-pointer executes (enqueue on `st`).
+cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, float* out_re,
+                     float* out_im, long long batch, long long in_dist, long long out_dist,
+                     bool interleaved, const float* window, cudaStream_t st);
+cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long long batch,
+                     long long in_dist, long long out_dist, bool interleaved, cudaStream_t st);
+cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, long long batch,
+                     long long in_dist, long long out_dist, bool interleaved, cudaStream_t st);
+cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long batch,
+                          long long in_dist, long long out_dist, const fafk::PipeOp* ops,
+                          int nops, cudaStream_t st);
+cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long long n_sig,
+                      long long sig_len, long long frames, bool interleaved, cudaStream_t st);
+
+// Host FFT in double precision (table generation only).
+void host_dft_fp64(std::vector<double>& re, std::vector<double>& im);
+
+}  // namespace fafp

@@ -1,0 +1,80 @@
+/*
+ * faf_cuda.h -- additive GPU entry points of the B200 transform path.
+ *
+ * Nothing here replaces a reference symbol; everything is new ABI that a
+ * GPU-aware caller may use on top of fastandfourier.h:
+ *
+ *   - streams: faf_cuda_set_stream / faf_cuda_synchronize
+ *   - batched execute: many transforms of one plan in one launch
+ *   - uneven batches: transforms of different lengths in one persistent,
+ *     CUDA-graph-captured launch (faf_uneven_*)
+ *   - serving: a continuous-batching request loop (faf_server_*)
+ *
+ * Pointers are plain `void *` / `float *` so the header needs no CUDA
+ * include; a `void *stream` is a cudaStream_t.
+ */
+#ifndef FAF_CUDA_H
+#define FAF_CUDA_H
+
+#include "fastandfourier.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- library / device --------------------------------------------------- */
+
+/* 1 if a CUDA device is usable, 0 otherwise (message in faf_get_error()). */
+int faf_cuda_available(void);
+/* Name of the plan kind behind t ("c2c", "rader", "bluestein", "r2c", "c2r",
+ * "pipeline", "stft", "c2c-4step", ...), or NULL. */
+const char *faf_cuda_plan_kind(const faf_transform *t);
+/* Number of kernel launches the last execute on this thread made. */
+int faf_cuda_last_launches(void);
+
+/* ---- streams ------------------------------------------------------------ */
+
+/* Enqueue this transform's work on `stream` (a cudaStream_t).  With a stream
+ * set, faf_execute on device buffers returns without synchronising.  NULL
+ * restores the default (legacy stream, synchronous execute). */
+int faf_cuda_set_stream(faf_transform *t, void *stream);
+void *faf_cuda_get_stream(const faf_transform *t);
+int faf_cuda_synchronize(const faf_transform *t);
+
+/* ---- batched execute ------------------------------------------------------ */
+
+/* Run `batch` transforms of plan t.  Transform b reads in->re + b*in_dist
+ * (and in->im + b*in_dist) and writes out->re + b*out_dist (...), distances
+ * counted in elements of one plane (complex elements for INTERLEAVED).
+ * A distance of 0 means "packed": the buffer's own logical length n.
+ * in / out describe ONE transform (same validation as faf_execute).
+ * Buffers are all device or all host memory; host buffers are copied in and
+ * out inside the call. */
+int faf_execute_batched(const faf_transform *t, faf_buffer *out, const faf_buffer *in,
+                        size_t batch, size_t in_dist, size_t out_dist);
+
+/* ---- uneven batches (one persistent launch) ------------------------------- */
+
+typedef struct faf_uneven faf_uneven;
+
+/* Plan `count` C2C transforms of the given lengths (each a legal
+ * faf_create_fft size <= 65536).  cfg supplies dir / norm / flags; n is
+ * ignored.  The ragged split-plane layout is packed: transform i starts at
+ * element offset sum_{j<i} lengths[j] in every plane. */
+faf_uneven *faf_uneven_create(const size_t *lengths, size_t count, const faf_config *cfg);
+/* Persistent, CUDA-graph-captured launch over all transforms (device
+ * pointers, enqueued on the plan's stream). */
+int faf_uneven_execute(faf_uneven *u, float *out_re, float *out_im, const float *in_re,
+                       const float *in_im);
+/* Reference GPU method: one launch per distinct length. */
+int faf_uneven_execute_plain(faf_uneven *u, float *out_re, float *out_im, const float *in_re,
+                             const float *in_im);
+int faf_uneven_set_stream(faf_uneven *u, void *stream);
+size_t faf_uneven_total(const faf_uneven *u);  /* total complex elements */
+void faf_uneven_destroy(faf_uneven *u);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FAF_CUDA_H */

@@ -1,0 +1,250 @@
+/*
+ * ref_driver.c -- batched, multi-threaded driver around the UNMODIFIED
+ * reference library (NotoriousLOB/FastAndFourier), compiled from its own
+ * sources by oracle/Makefile into oracle/_ref/libfaf_ref_<isa>.so.
+ *
+ * TEST / BASELINE INFRASTRUCTURE ONLY.  This file is linked into the
+ * reference build, never into the product library.  It is used by
+ *   - tests/golden/gen_golden.py   (golden fixtures from the reference),
+ *   - tests/ (validating the C restatement in oracle/faf_oracle.c),
+ *   - bench.py --impl reference / cpu_baseline (timing the reference on the
+ *     host cores).
+ *
+ * The reference transforms are not re-entrant (per-transform scratch,
+ * include/fastandfourier.h:490 `scratch`; src/faf_fft_splitradix.c:523 uses
+ * twiddles[1] as recursion work), so every worker thread creates its own
+ * transform objects and runs a contiguous slice of the batch through the
+ * reference's public faf_execute (include/fastandfourier.h:950).
+ */
+#define _GNU_SOURCE
+#include <pthread.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "fastandfourier.h"
+#include "chirp.h"
+
+/* Internal reference symbol (src/faf_twiddles.c:159), declared in faf.h. */
+void faf_gen_hann_window_f32(float *win, size_t n);
+
+static char g_drv_err[512];
+
+const char *refdrv_error(void) { return g_drv_err; }
+
+static void drv_fail(const char *what) {
+    snprintf(g_drv_err, sizeof(g_drv_err), "%s: %s", what, faf_get_error());
+}
+
+typedef enum { JOB_C2C, JOB_R2C, JOB_C2R, JOB_PIPE, JOB_STFT } job_kind;
+
+typedef struct {
+    job_kind kind;
+    size_t n;          /* transform length (FFT size for STFT) */
+    int inverse;
+    int norm;
+    uint32_t flags;
+    const char *src;   /* Chirp source (pipeline) */
+    const float *h_re, *h_im;
+    size_t h_bins;
+    size_t win, hop, sig_len, frames; /* STFT framing */
+    size_t b0, b1;     /* batch slice [b0, b1) */
+    const float *in_re, *in_im;
+    float *out_re, *out_im;
+    int rc;
+} job;
+
+static faf_transform *make_transform(const job *j) {
+    faf_config c = faf_config_init(j->n);
+    c.norm = (faf_norm)j->norm;
+    c.flags = j->flags;
+    switch (j->kind) {
+    case JOB_C2C:
+        c.layout = FAF_LAYOUT_SPLIT;
+        c.dir = j->inverse ? FAF_DIR_INVERSE : FAF_DIR_FORWARD;
+        return faf_create_fft(&c);
+    case JOB_R2C:
+    case JOB_STFT:
+        c.dir = FAF_DIR_FORWARD;
+        return faf_create_rfft(&c);
+    case JOB_C2R:
+        c.dir = FAF_DIR_INVERSE;
+        return faf_create_rfft(&c);
+    case JOB_PIPE: {
+        faf_transform *t = chirp_compile(j->src);
+        if (t && j->h_re) {
+            if (chirp_bind(t, "H", (void *)j->h_re, (void *)j->h_im, j->h_bins) != 0) {
+                faf_destroy_transform(t);
+                return NULL;
+            }
+        }
+        return t;
+    }
+    }
+    return NULL;
+}
+
+static void *run_job(void *arg) {
+    job *j = (job *)arg;
+    j->rc = 0;
+    if (j->b0 >= j->b1) return NULL;
+    faf_transform *t = make_transform(j);
+    if (!t) { drv_fail("create"); j->rc = -1; return NULL; }
+    size_t n = j->n, nb = n / 2 + 1;
+    float *frame = NULL;
+    float *win = NULL;
+    if (j->kind == JOB_STFT) {
+        frame = (float *)calloc(n, sizeof(float));
+        win = (float *)calloc(j->win, sizeof(float));
+        if (!frame || !win) { j->rc = -1; goto done; }
+        /* Reference symmetric Hann, src/faf_twiddles.c:159-163. */
+        faf_gen_hann_window_f32(win, j->win);
+    }
+    for (size_t b = j->b0; b < j->b1; b++) {
+        faf_buffer in, out;
+        int rc = 0;
+        switch (j->kind) {
+        case JOB_C2C:
+            in = faf_buffer_split((void *)(j->in_re + b * n), (void *)(j->in_im + b * n), n);
+            out = faf_buffer_split(j->out_re + b * n, j->out_im + b * n, n);
+            rc = faf_execute(t, &out, &in);
+            break;
+        case JOB_R2C:
+            in = faf_buffer_real((void *)(j->in_re + b * n), n);
+            out = faf_buffer_hermitian(j->out_re + b * nb, j->out_im + b * nb, nb);
+            rc = faf_execute(t, &out, &in);
+            break;
+        case JOB_C2R:
+            in = faf_buffer_hermitian((void *)(j->in_re + b * nb), (void *)(j->in_im + b * nb), nb);
+            out = faf_buffer_real(j->out_re + b * n, n);
+            rc = faf_execute(t, &out, &in);
+            break;
+        case JOB_PIPE:
+            in = faf_buffer_real((void *)(j->in_re + b * n), n);
+            out = faf_buffer_real(j->out_re + b * n, n);
+            rc = faf_execute(t, &out, &in);
+            break;
+        case JOB_STFT: {
+            /* Signal b, frame f: x[b*L + f*hop + i] * w[i] for i < win,
+             * zero-padded to n, then the reference R2C of n. */
+            size_t sig = b / j->frames, f = b % j->frames;
+            const float *x = j->in_re + sig * j->sig_len + f * j->hop;
+            for (size_t i = 0; i < j->win; i++) frame[i] = x[i] * win[i];
+            in = faf_buffer_real(frame, n);
+            out = faf_buffer_hermitian(j->out_re + b * nb, j->out_im + b * nb, nb);
+            rc = faf_execute(t, &out, &in);
+            break;
+        }
+        }
+        if (rc != 0) { drv_fail("execute"); j->rc = -1; break; }
+    }
+done:
+    free(frame);
+    free(win);
+    faf_destroy_transform(t);
+    return NULL;
+}
+
+static int run_batched(const job *proto, size_t batch, int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if ((size_t)nthreads > batch) nthreads = (int)(batch ? batch : 1);
+    job *jobs = (job *)calloc((size_t)nthreads, sizeof(job));
+    pthread_t *th = (pthread_t *)calloc((size_t)nthreads, sizeof(pthread_t));
+    if (!jobs || !th) { free(jobs); free(th); return -1; }
+    size_t per = batch / (size_t)nthreads, rem = batch % (size_t)nthreads, at = 0;
+    for (int i = 0; i < nthreads; i++) {
+        jobs[i] = *proto;
+        jobs[i].b0 = at;
+        at += per + ((size_t)i < rem ? 1 : 0);
+        jobs[i].b1 = at;
+    }
+    int rc = 0;
+    if (nthreads == 1) {
+        run_job(&jobs[0]);
+    } else {
+        for (int i = 0; i < nthreads; i++) pthread_create(&th[i], NULL, run_job, &jobs[i]);
+        for (int i = 0; i < nthreads; i++) pthread_join(th[i], NULL);
+    }
+    for (int i = 0; i < nthreads; i++) if (jobs[i].rc != 0) rc = -1;
+    free(jobs);
+    free(th);
+    return rc;
+}
+
+int refdrv_c2c(size_t n, int inverse, int norm, uint32_t flags, size_t batch,
+               const float *in_re, const float *in_im, float *out_re, float *out_im,
+               int nthreads) {
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_C2C; j.n = n; j.inverse = inverse; j.norm = norm; j.flags = flags;
+    j.in_re = in_re; j.in_im = in_im; j.out_re = out_re; j.out_im = out_im;
+    return run_batched(&j, batch, nthreads);
+}
+
+int refdrv_r2c(size_t n, int norm, size_t batch, const float *x,
+               float *out_re, float *out_im, int nthreads) {
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_R2C; j.n = n; j.norm = norm;
+    j.in_re = x; j.out_re = out_re; j.out_im = out_im;
+    return run_batched(&j, batch, nthreads);
+}
+
+int refdrv_c2r(size_t n, int norm, size_t batch, const float *in_re, const float *in_im,
+               float *y, int nthreads) {
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_C2R; j.n = n; j.norm = norm; j.inverse = 1;
+    j.in_re = in_re; j.in_im = in_im; j.out_re = y;
+    return run_batched(&j, batch, nthreads);
+}
+
+int refdrv_pipeline(const char *src, size_t n, const float *h_re, const float *h_im,
+                    size_t h_bins, size_t batch, const float *x, float *y, int nthreads) {
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_PIPE; j.n = n; j.src = src;
+    j.h_re = h_re; j.h_im = h_im; j.h_bins = h_bins;
+    j.in_re = x; j.out_re = y;
+    return run_batched(&j, batch, nthreads);
+}
+
+/* Framed real STFT over n_sig signals of sig_len samples each; output is
+ * [n_sig][frames][n/2+1] split planes, frames = 1 + (sig_len - win) / hop. */
+int refdrv_stft(size_t n, size_t win, size_t hop, size_t sig_len, size_t n_sig,
+                const float *x, float *out_re, float *out_im, int nthreads) {
+    if (win == 0 || win > n || hop == 0 || sig_len < win) {
+        snprintf(g_drv_err, sizeof(g_drv_err), "stft: bad framing");
+        return -1;
+    }
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_STFT; j.n = n; j.norm = FAF_NORM_NONE;
+    j.win = win; j.hop = hop; j.sig_len = sig_len;
+    j.frames = 1 + (sig_len - win) / hop;
+    j.in_re = x; j.out_re = out_re; j.out_im = out_im;
+    return run_batched(&j, n_sig * j.frames, nthreads);
+}
+
+/* Reference size policy, exposed for the parity tests of the planner. */
+int refdrv_is_size_supported(int type, size_t n) {
+    return faf_is_size_supported((faf_transform_type)type, n) ? 1 : 0;
+}
+
+size_t refdrv_recommended_size(int type, size_t n) {
+    return faf_get_recommended_size((faf_transform_type)type, n);
+}
+
+/* Create a C2C/R2C transform and report whether creation succeeded (for the
+ * create-time error tests); the message is copied into msg. */
+int refdrv_try_create(int type, size_t n, uint32_t flags, int layout, char *msg, size_t cap) {
+    faf_config c = faf_config_init(n);
+    c.flags = flags;
+    c.layout = (faf_layout)layout;
+    faf_clear_error();
+    faf_transform *t = faf_create((faf_transform_type)type, &c);
+    if (msg && cap) snprintf(msg, cap, "%s", faf_get_error());
+    if (!t) return 0;
+    faf_destroy_transform(t);
+    return 1;
+}

@@ -1,0 +1,158 @@
+"""ctypes bindings to the reference library itself (oracle/_ref/libfaf_ref_*.so),
+compiled from the reference's own C sources by `make -C oracle ref`.
+
+TEST / BASELINE INFRASTRUCTURE ONLY (see oracle/__init__.py).  Used to pin the
+C restatement, to generate golden fixtures (in the container that has the
+reference sources) and as the timed CPU baseline (`bench.py --impl
+reference`).  The library is prebuilt; the GPU host only loads it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_REF_DIR = os.path.join(_HERE, "_ref")
+REFERENCE_SRC = "/root/reference"
+_lib = None
+_isa = None
+_f32p = ctypes.POINTER(ctypes.c_float)
+
+
+def _cpu_has_avx512():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    fl = line.split()
+                    return "avx512f" in fl and "avx512bw" in fl and "avx512vl" in fl
+    except OSError:
+        pass
+    return False
+
+
+def isa():
+    return "v4" if _cpu_has_avx512() else "v3"
+
+
+def lib_path():
+    return os.path.join(_REF_DIR, f"libfaf_ref_{isa()}.so")
+
+
+def available():
+    return os.path.exists(lib_path())
+
+
+def build():
+    """Compile the reference library from its sources (needs the sources)."""
+    if not os.path.isdir(REFERENCE_SRC):
+        raise RuntimeError("reference sources not present; the prebuilt library "
+                           "must travel with the repository")
+    subprocess.run(["make", "-s", "-j8", "-C", _HERE, "ref", f"REF={REFERENCE_SRC}"],
+                   check=True)
+
+
+def lib():
+    global _lib, _isa
+    if _lib is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            build()
+        # The pipeline JIT writes under $HOME/.cache/fastandfourier.
+        os.environ.setdefault("HOME", "/tmp")
+        L = ctypes.CDLL(path)
+        sz, i, u32 = ctypes.c_size_t, ctypes.c_int, ctypes.c_uint32
+        L.refdrv_error.restype = ctypes.c_char_p
+        L.refdrv_c2c.argtypes = [sz, i, i, u32, sz, _f32p, _f32p, _f32p, _f32p, i]
+        L.refdrv_r2c.argtypes = [sz, i, sz, _f32p, _f32p, _f32p, i]
+        L.refdrv_c2r.argtypes = [sz, i, sz, _f32p, _f32p, _f32p, i]
+        L.refdrv_pipeline.argtypes = [ctypes.c_char_p, sz, _f32p, _f32p, sz, sz,
+                                      _f32p, _f32p, i]
+        L.refdrv_stft.argtypes = [sz, sz, sz, sz, sz, _f32p, _f32p, _f32p, i]
+        L.refdrv_is_size_supported.argtypes = [i, sz]
+        L.refdrv_recommended_size.argtypes = [i, sz]
+        L.refdrv_recommended_size.restype = sz
+        L.refdrv_try_create.argtypes = [i, sz, u32, i, ctypes.c_char_p, sz]
+        _lib = L
+        _isa = isa()
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(_f32p)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError("reference: " + lib().refdrv_error().decode())
+
+
+def c2c(re, im, inverse=False, norm=1, flags=0, threads=1):
+    re, im = _f32(re), _f32(im)
+    n = re.shape[-1]
+    yr, yi = np.empty_like(re), np.empty_like(im)
+    _check(lib().refdrv_c2c(n, int(inverse), norm, flags, re.size // n,
+                            _p(re), _p(im), _p(yr), _p(yi), threads))
+    return yr, yi
+
+
+def r2c(x, norm=1, threads=1):
+    x = _f32(x)
+    n = x.shape[-1]
+    shp = x.shape[:-1] + (n // 2 + 1,)
+    Xr, Xi = np.empty(shp, np.float32), np.empty(shp, np.float32)
+    _check(lib().refdrv_r2c(n, norm, x.size // n, _p(x), _p(Xr), _p(Xi), threads))
+    return Xr, Xi
+
+
+def c2r(Xr, Xi, n, norm=1, threads=1):
+    Xr, Xi = _f32(Xr), _f32(Xi)
+    y = np.empty(Xr.shape[:-1] + (n,), np.float32)
+    _check(lib().refdrv_c2r(n, norm, Xr.size // (n // 2 + 1), _p(Xr), _p(Xi), _p(y),
+                            threads))
+    return y
+
+
+def pipeline(src, x, hr=None, hi=None, threads=1):
+    x = _f32(x)
+    n = x.shape[-1]
+    y = np.empty_like(x)
+    hrp = hip = None
+    hb = 0
+    if hr is not None:
+        hr, hi = _f32(hr), _f32(hi)
+        hrp, hip, hb = _p(hr), _p(hi), hr.size
+    _check(lib().refdrv_pipeline(src.encode(), n, hrp, hip, hb, x.size // n,
+                                 _p(x), _p(y), threads))
+    return y
+
+
+def stft(x, n, win, hop, threads=1):
+    x = _f32(np.atleast_2d(x))
+    n_sig, L = x.shape
+    F = 1 + (L - win) // hop
+    shp = (n_sig, F, n // 2 + 1)
+    Xr, Xi = np.empty(shp, np.float32), np.empty(shp, np.float32)
+    _check(lib().refdrv_stft(n, win, hop, L, n_sig, _p(x), _p(Xr), _p(Xi), threads))
+    return Xr, Xi
+
+
+def is_size_supported(ttype, n):
+    return bool(lib().refdrv_is_size_supported(ttype, n))
+
+
+def recommended_size(ttype, n):
+    return int(lib().refdrv_recommended_size(ttype, n))
+
+
+def try_create(ttype, n, flags=0, layout=0):
+    buf = ctypes.create_string_buffer(512)
+    ok = lib().refdrv_try_create(ttype, n, flags, layout, buf, 512)
+    return bool(ok), buf.value.decode()
