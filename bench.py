@@ -1,0 +1,479 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 transform path (one JSON line on rank 0).
+
+Default workload: the fused real pipeline rfft(4096) -> raised-cosine notch
+(mul-spectrum, bins 400-420 with 32-bin ramps) -> irfft, FP32, batch 8192
+signals of N(0,1) noise + a 5-amplitude tone at bin 410 (seed 1).  One step
+is one pass of the fused pipeline kernel over the whole batch, inputs
+resident in HBM; the metric is algorithmic HBM GB/s (each input sample read
+once, each output sample written once: 8 bytes per sample) and its fraction
+of the measured HBM copy bandwidth.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload pipeline|r2c|c2c1024|c2c16384|stft]
+
+--impl reference times the reference library's own CPU path (compiled from
+its sources into oracle/_ref) on all host cores over a bounded sample of the
+same workload.  Under torchrun (N > 1) every rank runs its own batch (weak
+scaling, no collective on the data path); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+L2_BYTES = 126 * 1024 * 1024
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+
+def notch_mask(n=4096, lo=400, hi=420, ramp=32):
+    nb = n // 2 + 1
+    k = np.arange(nb)
+    m = np.ones(nb)
+    m[(k >= lo) & (k <= hi)] = 0.0
+    left = (k >= lo - ramp) & (k < lo)
+    m[left] = 0.5 * (1 + np.cos(np.pi * (k[left] - (lo - ramp)) / ramp))
+    right = (k > hi) & (k <= hi + ramp)
+    m[right] = 0.5 * (1 - np.cos(np.pi * (k[right] - hi) / ramp))
+    return m.astype(np.float32)
+
+
+WORKLOADS = {
+    # name: (description, n, batch, bytes per transform, flops per transform)
+    "pipeline": ("fused rfft(4096)->notch mul-spectrum->irfft, batch 8192, seed 1",
+                 4096, 8192, 8 * 4096, 2 * 2.5 * 4096 * 12),
+    "r2c": ("R2C n=4096 batch 8192, seed 1", 4096, 8192, 4 * 4096 + 8 * 2049, 2.5 * 4096 * 12),
+    "c2c1024": ("C2C n=1024 batch 256 forward (split planes), seed 0", 1024, 256,
+                16 * 1024, 5 * 1024 * 10),
+    "c2c16384": ("C2C n=16384 batch 2048 forward (split planes), seed 3", 16384, 2048,
+                 16 * 16384, 5 * 16384 * 14),
+    "stft": ("STFT Hann 1024 hop 256, 64 signals x 2^18 samples, seed 4", 1024, 64,
+             None, None),
+}
+
+
+def make_inputs(workload, batch):
+    n = WORKLOADS[workload][1]
+    if workload in ("pipeline", "r2c"):
+        rng = np.random.default_rng(1)
+        k = np.arange(n)
+        x = rng.standard_normal((batch, n), dtype=np.float32)
+        x += (5 * np.cos(2 * np.pi * 410 * k / n)).astype(np.float32)
+        return [x]
+    if workload.startswith("c2c"):
+        seed = 0 if workload == "c2c1024" else 3
+        rng = np.random.default_rng(seed)
+        re = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+        im = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+        if workload == "c2c16384":
+            for a in (re, im):
+                a[rng.random(a.shape) < 0.01] *= 1e3
+        return [re, im]
+    if workload == "stft":
+        rng = np.random.default_rng(4)
+        return [rng.standard_normal((batch, 1 << 18), dtype=np.float32)]
+    raise ValueError(workload)
+
+
+def stft_geometry(L, n=1024, win=1024, hop=256):
+    F = 1 + (L - win) // hop
+    return F, F * (n // 2 + 1)
+
+
+def algorithmic_bytes(workload, batch):
+    if workload == "stft":
+        L = 1 << 18
+        F, bins = stft_geometry(L)
+        return batch * (4 * L + 8 * bins)
+    return batch * WORKLOADS[workload][3]
+
+
+# ---------------------------------------------------------------------------
+# clocks (NVML, sampled during the timed region)
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        self._h = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._h = None
+
+    def _run(self):
+        nv = self._nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def __enter__(self):
+        if self._h is not None:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._h is not None:
+            self._t.join()
+
+    def result(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def measured_hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            v = json.load(f).get("hbm_gbs")
+        if v:
+            return float(v), "measured"
+    except Exception:
+        pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic(workload):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/<workload>.md, line `traffic_per_launch_bytes: X`)."""
+    p = os.path.join(ROOT, "profiles", f"{workload}.md")
+    try:
+        with open(p) as f:
+            for line in f:
+                if line.strip().startswith("traffic_per_launch_bytes:"):
+                    return float(line.split(":", 1)[1].strip().split()[0])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def build_transform(F, workload, torch):
+    n = WORKLOADS[workload][1]
+    if workload == "pipeline":
+        t = F.Transform.chirp(f"(pipeline (rfft :size {n}) (mul-spectrum) (irfft))")
+        m = torch.from_numpy(notch_mask(n)).cuda()
+        z = torch.zeros_like(m)
+        t.bind(m, z, n // 2 + 1)
+        return t
+    if workload == "r2c":
+        return F.Transform.rfft(n)
+    if workload.startswith("c2c"):
+        return F.Transform.fft(n)
+    if workload == "stft":
+        return F.Transform.stft(1024, win=1024, hop=256)
+    raise ValueError(workload)
+
+
+def run_step(F, t, workload, ins, outs):
+    if workload == "pipeline":
+        t.pipeline(ins[0], out=outs[0])
+    elif workload == "r2c":
+        t.r2c(ins[0], out_re=outs[0], out_im=outs[1])
+    elif workload.startswith("c2c"):
+        t.c2c(ins[0], ins[1], out_re=outs[0], out_im=outs[1])
+    elif workload == "stft":
+        t.stft_frames(ins[0], out_re=outs[0], out_im=outs[1])
+
+
+def alloc_outputs(workload, batch, like, torch):
+    n = WORKLOADS[workload][1]
+    dev = like.device if hasattr(like, "device") else None
+    mk = (lambda shp: torch.empty(shp, dtype=torch.float32, device=dev)) if dev is not None \
+        else (lambda shp: torch.empty(shp, dtype=torch.float32, pin_memory=True).numpy())
+    if workload == "pipeline":
+        return [mk((batch, n))]
+    if workload == "r2c":
+        return [mk((batch, n // 2 + 1)), mk((batch, n // 2 + 1))]
+    if workload.startswith("c2c"):
+        return [mk((batch, n)), mk((batch, n))]
+    if workload == "stft":
+        F_, bins = stft_geometry(1 << 18)
+        return [mk((batch, F_, 513)), mk((batch, F_, 513))]
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import fastandfourier_b200 as F
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    workload = args.workload
+    desc, n, batch, _, flops_per = WORKLOADS[workload]
+    host_in = make_inputs(workload, batch)
+    ins = [torch.from_numpy(a).cuda() for a in host_in]
+    outs = alloc_outputs(workload, batch, ins[0], torch)
+    t = build_transform(F, workload, torch)
+    stream = torch.cuda.current_stream()
+    t.set_stream(stream)
+    nbytes = algorithmic_bytes(workload, batch)
+
+    for _ in range(max(args.warmup, 3)):
+        run_step(F, t, workload, ins, outs)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            run_step(F, t, workload, ins, outs)
+            launches += F.lib().faf_cuda_last_launches()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        dist.barrier()
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_per_step = ms / args.steps
+    value = world * nbytes / (ms_per_step * 1e-3) / 1e9
+
+    # end to end through the public API with pinned host buffers
+    host_pinned = [torch.from_numpy(a).pin_memory().numpy() for a in host_in]
+    host_out = alloc_outputs(workload, batch, host_pinned[0], torch)
+    t_e2e = build_transform(F, workload, torch)
+    for _ in range(2):
+        run_step(F, t_e2e, workload, host_pinned, host_out)
+    e2e_steps = max(2, min(args.steps, 10))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        run_step(F, t_e2e, workload, host_pinned, host_out)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = sum(a.nbytes for a in host_pinned)
+    d2h = sum(a.nbytes for a in host_out)
+    e2e_value = world * nbytes / e2e_s / 1e9
+
+    peak, peak_kind = measured_hbm_peak()
+    achieved = nbytes / (ms_per_step * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": ncu_traffic(workload),
+                "algorithmic_bytes_per_launch": nbytes,
+                "kernel": {"pipeline": "k_pipeline", "r2c": "k_r2c", "stft": "k_stft"}.get(
+                    workload, "k_c2c")}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(workload, host_in, seconds=args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": "FFT GB/s (%HBM peak)",
+            "value": round(value, 1),
+            "unit": "GB/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(args.warmup, 3),
+            "ms_per_step": round(ms_per_step, 5),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded numpy PCG64)",
+            "config": {"workload": desc, "n": n, "batch_per_gpu": batch,
+                       "parallelism": f"replicas{world}",
+                       "l2": "inputs+outputs larger than L2 (no flush)"
+                       if nbytes > L2_BYTES else "L2-resident working set (launch-bound)"},
+            "pct_hbm_peak": round(100 * achieved / peak, 2),
+            "gflops_5nlog2n": round(world * batch * flops_per / (ms_per_step * 1e-3) / 1e9, 1)
+            if flops_per else None,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_s * 1e3, 3),
+                    "api": "faf_execute_batched with pinned host buffers"},
+            "gpu_launches": launches,
+            "clocks": sampler.result(),
+        }
+        print(json.dumps(line), flush=True)
+    t.close()
+    t_e2e.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# reference (CPU) arm
+# ---------------------------------------------------------------------------
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def _ref_call(refimpl, workload, sample_inputs, threads):
+    n = WORKLOADS[workload][1]
+    if workload == "pipeline":
+        m = notch_mask(n)
+        z = np.zeros_like(m)
+        refimpl.pipeline(f"(pipeline (rfft :size {n}) (mul-spectrum) (irfft))",
+                         sample_inputs[0], m, z, threads=threads)
+    elif workload == "r2c":
+        refimpl.r2c(sample_inputs[0], threads=threads)
+    elif workload.startswith("c2c"):
+        refimpl.c2c(sample_inputs[0], sample_inputs[1], threads=threads)
+    elif workload == "stft":
+        refimpl.stft(sample_inputs[0], 1024, 1024, 256, threads=threads)
+
+
+def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
+    """The reference library (oracle/_ref, built from its own sources) on the
+    host cores: repeat passes over a bounded sample until `seconds` elapse."""
+    from oracle import refimpl
+    if not refimpl.available():
+        try:
+            refimpl.build()
+        except Exception as e:  # the prebuilt library did not travel
+            return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
+                    "sample": f"unavailable: {e}"}
+    threads = threads or host_threads()
+    batch = host_in[0].shape[0]
+    sample_b = batch if workload != "stft" else max(1, min(batch, threads))
+    sample = [a[:sample_b] for a in host_in]
+    _ref_call(refimpl, workload, [a[:min(sample_b, threads)] for a in sample], threads)  # warm
+    nbytes = algorithmic_bytes(workload, sample_b)
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        _ref_call(refimpl, workload, sample, threads)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or reps >= 1000:
+            break
+    gbs = reps * nbytes / el / 1e9
+    return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
+            "isa": refimpl.isa(),
+            "sample": f"{reps} passes x {sample_b} transforms of the workload "
+                      f"({el:.1f} s, one faf_transform per thread)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    workload = args.workload
+    desc, n, batch, _, _ = WORKLOADS[workload]
+    host_in = make_inputs(workload, batch)
+    threads = host_threads()
+    from oracle import refimpl
+    if not refimpl.available():
+        try:
+            refimpl.build()
+        except Exception as e:
+            print(json.dumps({"impl": "reference", "unavailable": f"reference library missing: {e}"}))
+            return
+    # each step: a bounded sample of the workload (all host threads)
+    sample_b = min(batch, max(threads * 8, 64)) if workload != "stft" else min(batch, threads)
+    sample = [a[:sample_b] for a in host_in]
+    for _ in range(max(args.warmup, 1)):
+        _ref_call(refimpl, workload, sample, threads)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _ref_call(refimpl, workload, sample, threads)
+        times.append(time.perf_counter() - t0)
+    s = statistics.median(times)
+    nbytes = algorithmic_bytes(workload, sample_b)
+    gbs = nbytes / s / 1e9
+    line = {
+        "impl": "reference",
+        "metric": "FFT GB/s (%HBM peak)",
+        "value": round(gbs, 3),
+        "unit": "GB/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(s * 1e3, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded numpy PCG64)",
+        "config": {"workload": desc, "n": n, "batch_per_gpu": batch, "parallelism": "host cores"},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads,
+                         "kind": "reference", "isa": refimpl.isa(),
+                         "sample": f"{sample_b} of {batch} transforms per step, median of "
+                                   f"{args.steps} steps"},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pipeline", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if "WORLD_SIZE" not in os.environ:
+        world = 1
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -293,17 +293,25 @@ faf_transform* compile_pipeline(const Node* p) {
                  "in the middle");
             return nullptr;
         }
+    // Validate the whole form before any device plan is built.
+    const size_t nops = m1 - m0;
+    if (nops > (size_t)fafk::kMaxOps) {
+        fail("Chirp: at most %d spectral ops per fused pipeline", fafk::kMaxOps);
+        return nullptr;
+    }
+    std::vector<faf_inst> code(nops);
+    for (size_t i = 0; i < nops; i++)
+        if (emit_op(k[m0 + i].get(), &code[i]) != 0) return nullptr;
+    if (has_inv && tail->head == "inverse" && tail->kwarg("size")) {
+        fail("Chirp: (inverse) inherits size from the forward transform; delete :size "
+             "(inherited)");
+        return nullptr;
+    }
     faf_transform* fwd = compile_rfft(head, false);
     if (!fwd) return nullptr;
     faf_transform* inv = nullptr;
     if (has_inv) {
         if (tail->head == "inverse") {
-            if (tail->kwarg("size")) {
-                fail("Chirp: (inverse) inherits size from the forward transform; delete :size "
-                     "(inherited)");
-                faf_destroy_transform(fwd);
-                return nullptr;
-            }
             faf_config ic = faf_config_inverse(fwd->cfg);
             inv = faf_create_rfft(&ic);
         } else if (!tail->kwarg("size") && tail->kids.empty()) {
@@ -350,20 +358,10 @@ faf_transform* compile_pipeline(const Node* p) {
     }
     t->cfg.dir = has_inv ? FAF_DIR_INVERSE : FAF_DIR_FORWARD;
     t->flags = FAF_FLAG_REAL;
-    const size_t nops = m1 - m0;
-    if (nops > (size_t)fafk::kMaxOps) {
-        fail("Chirp: at most %d spectral ops per fused pipeline", fafk::kMaxOps);
-        faf_destroy_transform(t);
-        return nullptr;
-    }
     if (nops) {
         t->code = (faf_inst*)calloc(nops, sizeof(faf_inst));
         t->n_inst = nops;
-        for (size_t i = 0; i < nops; i++)
-            if (emit_op(k[m0 + i].get(), &t->code[i]) != 0) {
-                faf_destroy_transform(t);
-                return nullptr;
-            }
+        memcpy(t->code, code.data(), nops * sizeof(faf_inst));
     }
     // One fused kernel: forward norm of the R2C, inverse norm of the C2R.
     const faf_norm fn = fwd->cfg.norm;

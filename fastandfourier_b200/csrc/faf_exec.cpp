@@ -194,6 +194,9 @@ int execute_request(const faf_transform* t, Request& r) {
     DevicePlan* p = plan_of(t);
     if (!p) return fail("transform has no CUDA plan");
     if (r.batch <= 0) return 0;
+    // distance 0 = packed transforms
+    if (r.in_dist == 0) r.in_dist = (long long)r.in_len;
+    if (r.out_dist == 0) r.out_dist = (long long)r.out_len;
     int prev = -1;
     cudaGetDevice(&prev);
     if (prev != p->device) cudaSetDevice(p->device);

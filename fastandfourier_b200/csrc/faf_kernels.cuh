@@ -94,4 +94,12 @@ cudaError_t launch_rader(const fafd::Shape& S, const Geometry& g, const float2* 
 cudaError_t launch_bluestein(const fafd::Shape& S, const Geometry& g, const float2* tw,
                              const ConvArgs& a, cudaStream_t st);
 
+// Compile-time power-of-two kernels (k_pot2.cu).  kind: 0 = C2C (C2CArgs),
+// 1 = R2C, 2 = C2R, 3 = pipeline, 4 = STFT (RealArgs); log2n in [4, 14];
+// `tws` is the per-stage twiddle table of FftSize::d_tws.
+cudaError_t launch_pot2(int kind, int log2n, const float2* tws, const void* args,
+                        const Geometry& g, cudaStream_t st);
+// Shared-memory bytes the twiddle table of a log2n kernel adds to each CTA.
+size_t pot2_table_smem(int log2n);
+
 }  // namespace fafk

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 namespace fafp {
@@ -180,6 +181,31 @@ bool build_size(int n, FftSize& out, std::string& err) {
         !cuda_ok(upload(&out.d_stages, out.stages.data(), out.stages.size()), err,
                  "stage upload"))
         return false;
+    // FAF_CUDA_GENERIC=1 keeps power-of-two sizes on the runtime-radix
+    // kernels (both engines stay covered by the parity tests).
+    const char* gen = std::getenv("FAF_CUDA_GENERIC");
+    const bool force_generic = gen && gen[0] == '1';
+    if (!force_generic && n >= 16 && n <= kMaxSingleCta && (n & (n - 1)) == 0) {
+        // Per-stage table for the compile-time kernels: radix-16 stages, then
+        // the 8/4/2 remainder; stage s (s >= 1) with span P and radix R holds
+        // W_{PR}^{r k} at [(r - 1) P + k].
+        int lg = 0;
+        while ((1 << lg) < n) lg++;
+        const int n16 = lg / 4, rem = lg % 4, ns = n16 + (rem ? 1 : 0);
+        std::vector<float2> tws;
+        for (int s = 1; s < ns; s++) {
+            const int R = s < n16 ? 16 : (1 << rem), P = 1 << (4 * s);
+            for (int r = 1; r < R; r++)
+                for (int k = 0; k < P; k++) {
+                    const double a = -2.0 * M_PI * (double)r * (double)k / (double)(P * R);
+                    tws.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+                }
+        }
+        if (tws.empty()) tws.push_back(make_float2(1.f, 0.f));
+        if (!cuda_ok(upload(&out.d_tws, tws.data(), tws.size()), err, "twiddle upload"))
+            return false;
+        out.ct_log2 = lg;
+    }
     if (out.stages.empty()) {
         // n == 1: keep a valid pointer for the kernels.
         fafd::Stage dummy{1, 1, 1, 0};
@@ -191,8 +217,28 @@ bool build_size(int n, FftSize& out, std::string& err) {
 void free_size(FftSize& s) {
     cudaFree(s.d_stages);
     cudaFree(s.d_tw);
+    cudaFree(s.d_tws);
     s.d_stages = nullptr;
     s.d_tw = nullptr;
+    s.d_tws = nullptr;
+}
+
+// Geometry of the compile-time kernels: interleaved float2 workspace with one
+// pad element per 16 (plane2), T = n / 16 threads per transform, about 512
+// threads per CTA.
+fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch) {
+    fafk::Geometry g;
+    g.E = kE;
+    const int T = s.n / 16;
+    const size_t per = (size_t)((slots - 1) + ((slots - 1) >> 4) + 1) * sizeof(float2);
+    const size_t table = fafk::pot2_table_smem(s.ct_log2);
+    int G = std::max(1, 512 / T);
+    G = (int)std::min<long long>(G, std::max(1LL, batch));
+    while (G > 1 && ((size_t)G * per + table > kMaxSmem || G * T > 1024)) G--;
+    g.G = G;
+    g.threads = G * T;
+    g.smem = (size_t)G * per;
+    return g;
 }
 
 fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long batch) {
@@ -374,8 +420,9 @@ DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err) {
     p->kind = Kind::STFT;
     p->win = win;
     p->hop = hop;
-    // Symmetric Hann, reference src/faf_twiddles.c:159-163.
-    std::vector<float> w(std::max(win, 1));
+    // Symmetric Hann of win samples, zero-padded to n (the single-frame C2C
+    // path reads n entries), reference src/faf_twiddles.c:159-163.
+    std::vector<float> w(std::max(n, 1), 0.0f);
     for (int i = 0; i < win; i++)
         w[i] = win > 1 ? (float)(0.5 * (1.0 - std::cos(2.0 * M_PI * (double)i / (double)(win - 1))))
                        : 1.0f;
@@ -401,6 +448,9 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         a.scale = p->scale; a.sgn = sgn; a.interleaved = interleaved ? 1 : 0;
         a.window = window;
         const int slots = p->inner.n;
+        if (p->inner.ct_log2)
+            return fafk::launch_pot2(0, p->inner.ct_log2, p->inner.d_tws, &a,
+                                     geometry_ct(p->inner, slots, batch), st);
         return fafk::launch_c2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                                 p->inner.d_tw, a, st);
     }
@@ -436,6 +486,9 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
     a.in_a = x; a.out_a = Xr; a.out_b = Xi;
     a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
     const int slots = p->inner.n + 1;
+    if (p->inner.ct_log2)
+        return fafk::launch_pot2(1, p->inner.ct_log2, p->inner.d_tws, &a,
+                                 geometry_ct(p->inner, slots, batch), st);
     return fafk::launch_r2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);
 }
@@ -446,6 +499,9 @@ cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, 
     a.in_a = Xr; a.in_b = Xi; a.out_a = y;
     a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
     const int slots = p->inner.n + 1;
+    if (p->inner.ct_log2)
+        return fafk::launch_pot2(2, p->inner.ct_log2, p->inner.d_tws, &a,
+                                 geometry_ct(p->inner, slots, batch), st);
     return fafk::launch_c2r(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);
 }
@@ -460,6 +516,9 @@ cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long bat
     a.nops = std::min(nops, fafk::kMaxOps);
     for (int i = 0; i < a.nops; i++) a.ops[i] = ops[i];
     const int slots = p->inner.n + 1;
+    if (p->inner.ct_log2)
+        return fafk::launch_pot2(3, p->inner.ct_log2, p->inner.d_tws, &a,
+                                 geometry_ct(p->inner, slots, batch), st);
     return fafk::launch_pipeline(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                                  p->inner.d_tw, a, st);
 }
@@ -474,6 +533,9 @@ cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long 
     a.window = p->d_window; a.win = p->win; a.hop = p->hop;
     a.sig_len = sig_len; a.frames = frames;
     const int slots = p->inner.n + 1;
+    if (p->inner.ct_log2)
+        return fafk::launch_pot2(4, p->inner.ct_log2, p->inner.d_tws, &a,
+                                 geometry_ct(p->inner, slots, batch), st);
     return fafk::launch_stft(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                              p->inner.d_tw, a, st);
 }

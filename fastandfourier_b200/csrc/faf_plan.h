@@ -30,6 +30,8 @@ struct FftSize {
     std::vector<fafd::Stage> stages;
     fafd::Stage* d_stages = nullptr;
     float2* d_tw = nullptr;   // W_n^i, i < n (forward), from FP64
+    int ct_log2 = 0;          // > 0: compile-time power-of-two kernels apply
+    float2* d_tws = nullptr;  // their per-stage table [stage][r-1][k] = W_{PR}^{rk}
     fafd::Shape shape(int slots) const;
 };
 
@@ -38,6 +40,7 @@ bool build_size(int n, FftSize& out, std::string& err);
 void free_size(FftSize& s);
 int plane_floats(int slots);
 fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long batch);
+fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch);
 
 enum class Kind {
     C2C,        // single-CTA C2C (5-smooth / codelet / 7-smooth inner sizes)

@@ -1,0 +1,199 @@
+// faf_pot2.cuh -- compile-time Stockham engine for power-of-two lengths.
+//
+// Same algorithm as faf_device.cuh (radix-16 stages, then one 8/4/2 stage;
+// sources / sinks fused into the first / last stage), but with the length
+// fixed at compile time, so every span, mask, butterfly count and offset is
+// a constant, and with the working set stored as interleaved complex float2
+// in shared memory (one 64-bit access per element, one pad element per 16:
+// conflict-free for the stride-16 first-stage stores).
+//
+// Twiddles live in a per-stage table laid out [stage][r-1][k]: for stage s
+// with span P and radix R, entry (r, k) = W_{P R}^{r k}.  Lanes of a warp hold
+// consecutive k, so every twiddle load of a warp is one contiguous segment.
+#pragma once
+
+#include <type_traits>
+
+#include "faf_device.cuh"
+
+namespace fafct {
+
+using fafd::cf;
+using fafd::cmul_inplace;
+using fafd::Dft;
+
+__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+
+template <int N>
+struct P2 {
+    static_assert(N >= 16 && (N & (N - 1)) == 0, "power of two >= 16");
+    static constexpr int LOG = ilog2(N);
+    static constexpr int N16 = LOG / 4;
+    static constexpr int REM = LOG % 4;
+    static constexpr int NS = N16 + (REM ? 1 : 0);
+    static constexpr int T = N / 16;                    // threads per transform
+    __host__ __device__ static constexpr int radix(int s) { return s < N16 ? 16 : (1 << REM); }
+    __host__ __device__ static constexpr int span(int s) { return 1 << (4 * s); }
+    __host__ __device__ static constexpr int tw_offset(int s) {
+        int o = 0;
+        for (int j = 1; j < s; j++) o += (radix(j) - 1) * span(j);
+        return o;
+    }
+    static constexpr int TW = tw_offset(NS);            // table entries
+};
+
+__device__ __forceinline__ int pad2(int a) { return a + (a >> 4); }
+
+// float2 slots needed for `slots` complex elements
+__host__ __device__ constexpr int plane2(int slots) {
+    return (slots - 1) + ((slots - 1) >> 4) + 1;
+}
+
+// Interleaved complex workspace.  kFast marks shared-memory sources / sinks
+// whose strided accesses the stage turns into one padded base address plus
+// compile-time offsets.
+struct SmemC {
+    float2* d;
+    static constexpr bool kSmem = true;
+    static constexpr bool kFast = true;
+    static constexpr bool kConj = false;
+    __device__ __forceinline__ cf get(int i) const {
+        const float2 v = d[pad2(i)];
+        return cf{v.x, v.y};
+    }
+    __device__ __forceinline__ void put(int i, cf v) const { d[pad2(i)] = make_float2(v.x, v.y); }
+};
+
+struct SmemCConj {
+    float2* d;
+    static constexpr bool kSmem = true;
+    static constexpr bool kFast = true;
+    static constexpr bool kConj = true;
+    __device__ __forceinline__ cf get(int i) const {
+        const float2 v = d[pad2(i)];
+        return cf{v.x, -v.y};
+    }
+};
+
+template <class T, class = void>
+struct is_fast : std::false_type {};
+template <class T>
+struct is_fast<T, std::void_t<decltype(T::kFast)>> : std::bool_constant<T::kFast> {};
+
+template <class Snk>
+struct LastC {
+    Snk s;
+    static constexpr bool kSmem = false;
+    static constexpr bool kFast = is_fast<Snk>::value;
+    __device__ __forceinline__ void put(int i, cf v) const { s.put(i, v); }
+};
+
+template <class T>
+__device__ __forceinline__ float2* fast_ptr(const T& x) {
+    if constexpr (std::is_same_v<T, SmemC> || std::is_same_v<T, SmemCConj>) return x.d;
+    else return x.s.d;
+}
+
+template <int N, int S, bool TWS_SMEM, class Src, class Snk>
+__device__ __forceinline__ void ct_stage(float (&xr)[16], float (&xi)[16], int t,
+                                         const float2* __restrict__ tws, const Src& src,
+                                         const Snk& snk) {
+    using Pl = P2<N>;
+    constexpr int R = Pl::radix(S), P = Pl::span(S), NB = N / R, T = Pl::T, MB = 16 / R;
+    constexpr int LP = ilog2(P);
+    constexpr int OFF = Pl::tw_offset(S);
+#pragma unroll
+    for (int i = 0; i < MB; i++) {
+        const int b = t + i * T;
+        if constexpr (is_fast<Src>::value && NB % 16 == 0) {
+            // pad2(b + r NB) = pad2(b) + r (NB + NB / 16)
+            const float2* p = fast_ptr(src) + pad2(b);
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const float2 v = p[r * (NB + NB / 16)];
+                xr[i * R + r] = v.x;
+                xi[i * R + r] = Src::kConj ? -v.y : v.y;
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const cf v = src.get(b + r * NB);
+                xr[i * R + r] = v.x;
+                xi[i * R + r] = v.y;
+            }
+        }
+        if constexpr (S > 0) {
+            const int k = b & (P - 1);
+            const float2* w = tws + OFF + k;
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                const float2 wr = TWS_SMEM ? w[(r - 1) * P] : __ldg(&w[(r - 1) * P]);
+                cmul_inplace(xr[i * R + r], xi[i * R + r], wr.x, wr.y);
+            }
+        }
+        Dft<R>::run(&xr[i * R], &xi[i * R]);
+    }
+    if constexpr (Src::kSmem && Snk::kSmem) __syncthreads();
+#pragma unroll
+    for (int i = 0; i < MB; i++) {
+        const int b = t + i * T;
+        const int k = b & (P - 1);
+        const int base = ((b >> LP) << (LP + ilog2(R))) + k;
+        if constexpr (is_fast<Snk>::value && (P % 16 == 0 || (P == 1 && R == 16))) {
+            // P % 16 == 0: pad2(base + r P) = pad2(base) + r (P + P / 16);
+            // P == 1, R == 16: base = 16 b, pad2(16 b + r) = 17 b + r.
+            float2* p = fast_ptr(snk) + pad2(base);
+            constexpr int step = (P % 16 == 0) ? P + P / 16 : 1;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int j = i * R + Dft<R>::slot(r);
+                p[r * step] = make_float2(xr[j], xi[j]);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int j = i * R + Dft<R>::slot(r);
+                snk.put(base + r * P, cf{xr[j], xi[j]});
+            }
+        }
+    }
+    if constexpr (Snk::kSmem) __syncthreads();
+}
+
+template <int N, int S, bool TWS_SMEM, class Src, class Snk>
+__device__ __forceinline__ void ct_run(float (&xr)[16], float (&xi)[16], int t, float2* ws,
+                                       const float2* __restrict__ tws, const Src& src,
+                                       const Snk& snk) {
+    using Pl = P2<N>;
+    const SmemC mid{ws};
+    const LastC<Snk> last{snk};
+    if constexpr (Pl::NS == 1) {
+        if constexpr (Src::kSmem) {
+            ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid);
+            for (int i = t; i < N; i += Pl::T) last.put(i, mid.get(i));
+        } else {
+            ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, last);
+        }
+    } else if constexpr (S == 0) {
+        ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid);
+        ct_run<N, 1, TWS_SMEM>(xr, xi, t, ws, tws, mid, snk);
+    } else if constexpr (S == Pl::NS - 1) {
+        ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, last);
+    } else {
+        ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, mid);
+        ct_run<N, S + 1, TWS_SMEM>(xr, xi, t, ws, tws, mid, snk);
+    }
+}
+
+// Forward FFT of N points (compile time) by the T = N/16 threads of one
+// transform group; `ws` is the group's interleaved workspace, `tws` the
+// per-stage twiddle table (shared memory when TWS_SMEM, else global).
+template <int N, bool TWS_SMEM, class Src, class Snk>
+__device__ __forceinline__ void ct_fft(int t, float2* ws, const float2* __restrict__ tws,
+                                       const Src& src, const Snk& snk) {
+    float xr[16], xi[16];
+    if constexpr (!Src::kSmem) __syncthreads();
+    ct_run<N, 0, TWS_SMEM>(xr, xi, t, ws, tws, src, snk);
+}
+
+}  // namespace fafct

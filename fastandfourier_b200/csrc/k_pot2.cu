@@ -1,0 +1,358 @@
+// k_pot2.cu -- C2C, R2C, C2R, fused pipeline and STFT kernels for
+// power-of-two inner lengths 16..16384 on the compile-time engine
+// (faf_pot2.cuh).  Same sources / sinks and the same reference semantics as
+// the generic kernels; one instantiation per length.
+//
+// The kernels are persistent: the grid is sized to the resident CTAs and
+// each CTA walks transform groups c, c + grid, ...  The per-stage twiddle
+// table is copied into shared memory once per CTA when it fits in 32 KB.
+#include <algorithm>
+
+#include "faf_kernels_common.cuh"
+#include "faf_pot2.cuh"
+
+namespace fafk {
+
+using fafct::P2;
+using fafct::SmemC;
+using fafct::SmemCConj;
+using fafct::ct_fft;
+using fafct::plane2;
+
+// Shared-memory layout of one CTA:
+//   [twiddle table, if it fits 32 KB] [group 0 workspace] [group 1 ...] ...
+template <int N>
+struct CtCfg {
+    static constexpr bool TW_SMEM = P2<N>::TW * 8 <= 32768;
+    static constexpr int TWN = TW_SMEM ? (P2<N>::TW > 0 ? P2<N>::TW : 1) : 0;
+};
+
+template <int N>
+struct CtGroup {
+    int g, t;
+    float2* ws;
+    const float2* tw;
+    // Every kernel body begins with a barrier, which publishes the table.
+    __device__ __forceinline__ CtGroup(float2* sm, int slots, const float2* __restrict__ gtw) {
+        constexpr int T = P2<N>::T;
+        g = threadIdx.x / T;
+        t = threadIdx.x % T;
+        if constexpr (CtCfg<N>::TW_SMEM) {
+            for (int i = threadIdx.x; i < CtCfg<N>::TWN; i += blockDim.x) sm[i] = __ldg(&gtw[i]);
+            tw = sm;
+        } else {
+            tw = gtw;
+        }
+        ws = sm + CtCfg<N>::TWN + (size_t)g * plane2(slots);
+    }
+};
+
+template <int N>
+constexpr bool kTw = CtCfg<N>::TW_SMEM;
+
+// Persistent loop over transform groups; uniform across the CTA.
+#define CT_FOR_GROUPS(G, batch)                                                          \
+    for (long long grp_ = blockIdx.x, ngrp_ = ((batch) + (G)-1) / (G); grp_ < ngrp_;     \
+         grp_ += gridDim.x)
+
+template <int N>
+__global__ void __launch_bounds__(1024) k2_c2c(const float2* __restrict__ tws, const C2CArgs a,
+                                               int G) {
+    extern __shared__ float4 smem4[];
+    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N, tws);
+    const int fpe = a.interleaved ? 2 : 1;
+    CT_FOR_GROUPS(G, a.batch) {
+        const long long b = grp_ * G + q.g;
+        const bool live = b < a.batch;
+        const long long bi = live ? b : 0;
+        const long long io = bi * a.in_dist * fpe, oo = bi * a.out_dist * fpe;
+        SplitSrc src{a.in_re + io, a.interleaved ? nullptr : a.in_im + io, a.window, a.sgn,
+                     a.interleaved, live};
+        SplitSink snk{a.out_re + oo, a.interleaved ? nullptr : a.out_im + oo, a.scale, a.sgn,
+                      a.interleaved, live};
+        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, src, snk);  // begins with a barrier
+    }
+}
+
+// Post-pass over bin pairs after the forward FFT left Z in the workspace.
+template <int N>
+__device__ __forceinline__ void ct_r2c_post(int t, const SmemC& mid,
+                                            const float2* __restrict__ stw, const HermSink& out,
+                                            float scale) {
+    constexpr int nc = N;
+    for (int k = t; k <= nc / 2; k += P2<N>::T) {
+        if (k == 0) {
+            const cf z = mid.get(0);
+            out.put(0, (z.x + z.y) * scale, 0.f);
+            out.put(nc, (z.x - z.y) * scale, 0.f);
+        } else {
+            cf Xk, Xnk;
+            r2c_pair(mid.get(k), mid.get(nc - k), __ldg(&stw[k - 1]), Xk, Xnk);
+            if (k != nc - k) out.put(k, Xk.x * scale, Xk.y * scale);
+            out.put(nc - k, Xnk.x * scale, Xnk.y * scale);
+        }
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, const RealArgs a,
+                                               int G, bool vec) {
+    extern __shared__ float4 smem4[];
+    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws);
+    const SmemC mid{q.ws};
+    const int fpe = a.interleaved ? 2 : 1;
+    CT_FOR_GROUPS(G, a.batch) {
+        const long long b = grp_ * G + q.g;
+        const bool live = b < a.batch;
+        const long long bi = live ? b : 0;
+        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid);
+        __syncthreads();
+        if (live) {
+            const long long oo = bi * a.out_dist * fpe;
+            HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo, a.interleaved};
+            ct_r2c_post<N>(q.t, mid, a.stw, out, a.scale);
+        }
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(1024) k2_stft(const float2* __restrict__ tws, const RealArgs a,
+                                                int G) {
+    extern __shared__ float4 smem4[];
+    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws);
+    const SmemC mid{q.ws};
+    const int fpe = a.interleaved ? 2 : 1;
+    CT_FOR_GROUPS(G, a.batch) {
+        const long long b = grp_ * G + q.g;  // global frame index
+        const bool live = b < a.batch;
+        const long long bi = live ? b : 0;
+        const long long sig = bi / a.frames, f = bi - sig * a.frames;
+        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw,
+                          FrameSrc{a.in_a + sig * a.sig_len + f * a.hop, a.window, a.win, live},
+                          mid);
+        __syncthreads();
+        if (live) {
+            const long long oo = bi * a.out_dist * fpe;
+            HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo, a.interleaved};
+            ct_r2c_post<N>(q.t, mid, a.stw, out, a.scale);
+        }
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, const RealArgs a,
+                                               int G, bool vec) {
+    extern __shared__ float4 smem4[];
+    constexpr int nc = N, T = P2<N>::T;
+    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws);
+    const SmemC mid{q.ws};
+    const int fpe = a.interleaved ? 2 : 1;
+    CT_FOR_GROUPS(G, a.batch) {
+        const long long b = grp_ * G + q.g;
+        const bool live = b < a.batch;
+        const long long bi = live ? b : 0;
+        const long long io = bi * a.in_dist * fpe;
+        __syncthreads();  // the previous transform's last stage may still read ws
+        for (int k = q.t; k <= nc; k += T) {
+            cf v{0.f, 0.f};
+            if (live) {
+                if (a.interleaved) {
+                    const float2 u = __ldcs(reinterpret_cast<const float2*>(a.in_a + io) + k);
+                    v = cf{u.x, u.y};
+                } else {
+                    v = cf{__ldcs(a.in_a + io + k), __ldcs(a.in_b + io + k)};
+                }
+            }
+            mid.put(k, v);
+        }
+        __syncthreads();
+        for (int k = q.t; k <= nc / 2; k += T) {
+            if (k == 0) {
+                const cf x0 = mid.get(0), xn = mid.get(nc);
+                mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
+            } else {
+                cf Zk, Znk;
+                c2r_pair(mid.get(k), mid.get(nc - k), __ldg(&a.stw[k - 1]), Zk, Znk);
+                if (k != nc - k) mid.put(k, Zk);
+                mid.put(nc - k, Znk);
+            }
+        }
+        __syncthreads();
+        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
+                          RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec});
+    }
+}
+
+__device__ __forceinline__ cf apply_ops2(const RealArgs& a, int k, cf v) {
+#pragma unroll
+    for (int o = 0; o < kMaxOps; o++) {
+        if (o >= a.nops) break;
+        const PipeOp& op = a.ops[o];
+        if (op.code == OP_CONJ) {
+            v.y = -v.y;
+        } else if (op.code == OP_MUL) {
+            if (k < op.m) {
+                const float hr = __ldg(op.hr + k);
+                if (k == 0 || k == op.m - 1) {
+                    v = cf{v.x * hr, 0.f};
+                } else {
+                    const float hi = __ldg(op.hi_ + k);
+                    v = cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
+                }
+            }
+        } else if (op.code == OP_BANDPASS) {
+            if (k < op.lo || k > op.hi) v = cf{0.f, 0.f};
+        }
+    }
+    return v;
+}
+
+template <int N>
+__global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ tws,
+                                                    const RealArgs a, int G, bool vec) {
+    extern __shared__ float4 smem4[];
+    constexpr int nc = N, T = P2<N>::T;
+    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws);
+    const SmemC mid{q.ws};
+    CT_FOR_GROUPS(G, a.batch) {
+        const long long b = grp_ * G + q.g;
+        const bool live = b < a.batch;
+        const long long bi = live ? b : 0;
+        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid);
+        __syncthreads();
+        // Per bin pair: post-pass -> ops -> pre-pass, in registers.
+        for (int k = q.t; k <= nc / 2; k += T) {
+            if (k == 0) {
+                const cf z = mid.get(0);
+                const cf x0 = apply_ops2(a, 0, cf{z.x + z.y, 0.f});
+                const cf xn = apply_ops2(a, nc, cf{z.x - z.y, 0.f});
+                mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
+            } else {
+                const float2 w = __ldg(&a.stw[k - 1]);
+                cf Xk, Xnk;
+                r2c_pair(mid.get(k), mid.get(nc - k), w, Xk, Xnk);
+                if (k == nc - k) Xk = Xnk;
+                Xk = apply_ops2(a, k, Xk);
+                Xnk = (k == nc - k) ? Xk : apply_ops2(a, nc - k, Xnk);
+                cf Zk, Znk;
+                c2r_pair(Xk, Xnk, w, Zk, Znk);
+                if (k != nc - k) mid.put(k, Zk);
+                mid.put(nc - k, Znk);
+            }
+        }
+        __syncthreads();
+        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
+                          RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec});
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch by log2 length (persistent grid = resident CTAs, capped by work)
+// ---------------------------------------------------------------------------
+
+template <class K>
+static unsigned persistent_grid(K kernel, const Geometry& g, long long batch) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, g.threads, g.smem) !=
+            cudaSuccess ||
+        per_sm <= 0)
+        per_sm = 1;
+    const long long groups = (batch + g.G - 1) / g.G;
+    const long long cap = (long long)sms * per_sm;
+    return (unsigned)std::max(1LL, std::min(groups, cap));
+}
+
+template <int N>
+static size_t tw_bytes() {
+    return (size_t)CtCfg<N>::TWN * sizeof(float2);
+}
+
+template <int N>
+static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geometry g,
+                             cudaStream_t st) {
+    cudaError_t e;
+    g.smem += tw_bytes<N>();
+    switch (kind) {
+    case 0: {
+        const C2CArgs& a = *(const C2CArgs*)args;
+        if ((e = prep(k2_c2c<N>, g.smem)) != cudaSuccess) return e;
+        k2_c2c<N><<<persistent_grid(k2_c2c<N>, g, a.batch), g.threads, g.smem, st>>>(tws, a, g.G);
+        break;
+    }
+    case 1: {
+        const RealArgs& a = *(const RealArgs*)args;
+        if ((e = prep(k2_r2c<N>, g.smem)) != cudaSuccess) return e;
+        k2_r2c<N><<<persistent_grid(k2_r2c<N>, g, a.batch), g.threads, g.smem, st>>>(
+            tws, a, g.G, vec_ok(a.in_a, a.in_dist));
+        break;
+    }
+    case 2: {
+        const RealArgs& a = *(const RealArgs*)args;
+        if ((e = prep(k2_c2r<N>, g.smem)) != cudaSuccess) return e;
+        k2_c2r<N><<<persistent_grid(k2_c2r<N>, g, a.batch), g.threads, g.smem, st>>>(
+            tws, a, g.G, vec_ok(a.out_a, a.out_dist));
+        break;
+    }
+    case 3: {
+        const RealArgs& a = *(const RealArgs*)args;
+        if ((e = prep(k2_pipeline<N>, g.smem)) != cudaSuccess) return e;
+        k2_pipeline<N><<<persistent_grid(k2_pipeline<N>, g, a.batch), g.threads, g.smem, st>>>(
+            tws, a, g.G, vec_ok(a.in_a, a.in_dist) && vec_ok(a.out_a, a.out_dist));
+        break;
+    }
+    case 4: {
+        const RealArgs& a = *(const RealArgs*)args;
+        if ((e = prep(k2_stft<N>, g.smem)) != cudaSuccess) return e;
+        k2_stft<N><<<persistent_grid(k2_stft<N>, g, a.batch), g.threads, g.smem, st>>>(tws, a,
+                                                                                        g.G);
+        break;
+    }
+    default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+size_t pot2_table_smem(int log2n) {
+    switch (log2n) {
+    case 4: return tw_bytes<16>();
+    case 5: return tw_bytes<32>();
+    case 6: return tw_bytes<64>();
+    case 7: return tw_bytes<128>();
+    case 8: return tw_bytes<256>();
+    case 9: return tw_bytes<512>();
+    case 10: return tw_bytes<1024>();
+    case 11: return tw_bytes<2048>();
+    case 12: return tw_bytes<4096>();
+    case 13: return tw_bytes<8192>();
+    case 14: return tw_bytes<16384>();
+    default: return 0;
+    }
+}
+
+cudaError_t launch_pot2(int kind, int log2n, const float2* tws, const void* args,
+                        const Geometry& g, cudaStream_t st) {
+    switch (log2n) {
+    case 4: return ct_launch<16>(kind, tws, args, g, st);
+    case 5: return ct_launch<32>(kind, tws, args, g, st);
+    case 6: return ct_launch<64>(kind, tws, args, g, st);
+    case 7: return ct_launch<128>(kind, tws, args, g, st);
+    case 8: return ct_launch<256>(kind, tws, args, g, st);
+    case 9: return ct_launch<512>(kind, tws, args, g, st);
+    case 10: return ct_launch<1024>(kind, tws, args, g, st);
+    case 11: return ct_launch<2048>(kind, tws, args, g, st);
+    case 12: return ct_launch<4096>(kind, tws, args, g, st);
+    case 13: return ct_launch<8192>(kind, tws, args, g, st);
+    case 14: return ct_launch<16384>(kind, tws, args, g, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace fafk

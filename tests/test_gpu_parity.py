@@ -313,3 +313,17 @@ def test_config1_c2c_forward_inverse(cuda):
     wr, wi = orc.c2c(re, im)
     assert orc.rel_l2_complex(host(Yr), host(Yi), wr + 1j * wi) <= REL_L2_TOL
     assert orc.rel_l2_complex(host(Zr), host(Zi), re + 1j * im) <= REL_L2_TOL
+
+
+@pytest.mark.parametrize("n", [16, 64, 1024, 2048, 16384])
+def test_generic_engine_power_of_two(cuda, n, monkeypatch):
+    """The runtime-radix engine on power-of-two sizes (normally served by the
+    compile-time kernels) stays in parity too."""
+    import fastandfourier_b200 as F
+    monkeypatch.setenv("FAF_CUDA_GENERIC", "1")
+    _, e_orc, e_64 = _c2c_case(cuda, F, n, False)
+    assert e_orc <= REL_L2_TOL and e_64 <= REL_L2_TOL
+    torch = cuda
+    x = seeded(200 + n).standard_normal((3, 2 * n)).astype(np.float32)
+    Xr, Xi = F.Transform.rfft(2 * n).r2c(dev(torch, x))
+    assert orc.rel_l2_complex(host(Xr), host(Xi), orc.fp64_r2c(x)) <= REL_L2_TOL
