@@ -15,6 +15,7 @@ struct Geometry {
     int G;          // transforms per CTA
     int threads;    // G * T
     size_t smem;    // dynamic shared memory bytes
+    bool staged = false;  // power-of-two real-input kernels: cp.async input staging
 };
 
 // Spectral op codes used inside the fused pipeline kernel.
@@ -77,6 +78,22 @@ struct ConvArgs {  // Rader (prime n) and Bluestein (any n)
     const float2* B;       // FFT of the convolution kernel, inner length
     float inv_inner;       // 1 / inner length
 };
+
+// Four-step transforms longer than one CTA (k_large.cu).
+constexpr int kLargeThreads = 512;
+struct LargeArgs {
+    fafd::Shape s1, s2;    // N1 / N2 shapes, T padded to a divisor of kLargeThreads
+    int n1, n2;
+    const float2* tw1;     // N1-point twiddles
+    const float2* tw2;     // N2-point twiddles
+    const float2* twn;     // n-point twiddles (middle factors W_n^{n2 k1})
+    float* scratch;        // per-CTA scratch, cta_floats each
+    long long cta_floats;
+};
+// kind: 0 = C2C (C2CArgs), 1 = R2C, 2 = C2R, 3 = pipeline (RealArgs)
+cudaError_t launch_large(int kind, const LargeArgs& a, const void* args, long long batch,
+                         int grid, cudaStream_t st);
+size_t large_smem(const LargeArgs& a, int threads);
 
 // Host launchers (return a cudaError_t).  `S` is the inner FFT shape.
 cudaError_t launch_c2c(const fafd::Shape& S, const Geometry& g, const float2* tw,

@@ -232,4 +232,31 @@ inline bool vec_ok(const void* p, long long dist) {
     return (((unsigned long long)(size_t)p) % 8 == 0) && (dist % 2 == 0);
 }
 
+// Spectral ops of the fused pipeline on bin k (reference src/chirp.c:421-471,
+// src/faf_core.c:150-166): CONJ negates im; MUL multiplies by the bound H with
+// real DC and last-bin products; BANDPASS zeroes bins outside [lo, hi].
+__device__ __forceinline__ cf apply_pipe_ops(const RealArgs& a, int k, cf v) {
+#pragma unroll
+    for (int o = 0; o < kMaxOps; o++) {
+        if (o >= a.nops) break;
+        const PipeOp& op = a.ops[o];
+        if (op.code == OP_CONJ) {
+            v.y = -v.y;
+        } else if (op.code == OP_MUL) {
+            if (k < op.m) {
+                const float hr = __ldg(op.hr + k);
+                if (k == 0 || k == op.m - 1) {
+                    v = cf{v.x * hr, 0.f};
+                } else {
+                    const float hi = __ldg(op.hi_ + k);
+                    v = cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
+                }
+            }
+        } else if (op.code == OP_BANDPASS) {
+            if (k < op.lo || k > op.hi) v = cf{0.f, 0.f};
+        }
+    }
+    return v;
+}
+
 }  // namespace fafk

@@ -226,18 +226,29 @@ void free_size(FftSize& s) {
 // Geometry of the compile-time kernels: interleaved float2 workspace with one
 // pad element per 16 (plane2), T = n / 16 threads per transform, about 512
 // threads per CTA.
-fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch) {
+fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, bool staged,
+                           int target_threads) {
     fafk::Geometry g;
     g.E = kE;
     const int T = s.n / 16;
-    const size_t per = (size_t)((slots - 1) + ((slots - 1) >> 4) + 1) * sizeof(float2);
+    // same layout as k_pot2.cu: even2(plane2(slots)) [+ n] float2 per group
+    const int plane2 = (slots - 1) + ((slots - 1) >> 4) + 1;
     const size_t table = fafk::pot2_table_smem(s.ct_log2);
-    int G = std::max(1, 512 / T);
+    size_t per = (size_t)((plane2 + 1) & ~1) * sizeof(float2);
+    // staging adds n float2 per group; drop it when one group no longer fits
+    if (staged && per + (size_t)s.n * sizeof(float2) + table > kMaxSmem) staged = false;
+    if (staged) per += (size_t)s.n * sizeof(float2);
+    int target = target_threads;
+    if (const char* env = std::getenv("FAF_CUDA_CTA_THREADS")) target = std::max(1, atoi(env));
+    int G = std::max(1, target / T);
     G = (int)std::min<long long>(G, std::max(1LL, batch));
+    // groups of >= 32 threads synchronise on named barriers 1..15
+    if (T >= 32) G = std::min(G, 15);
     while (G > 1 && ((size_t)G * per + table > kMaxSmem || G * T > 1024)) G--;
     g.G = G;
     g.threads = G * T;
     g.smem = (size_t)G * per;
+    g.staged = staged;
     return g;
 }
 
@@ -246,12 +257,26 @@ fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long
     g.E = kE;
     const size_t per = (size_t)(2 * plane_floats(slots) + extra_floats) * sizeof(float);
     int G = std::max(1, kTargetThreads / s.T);
-    G = std::min<long long>(G, std::max(1LL, batch));
+    G = (int)std::min<long long>(G, std::max(1LL, batch));
     while (G > 1 && ((size_t)G * per > kMaxSmem || G * s.T > 1024)) G--;
     g.G = G;
     g.threads = G * s.T;
     g.smem = (size_t)G * per;
     return g;
+}
+
+// cp.async staging of a real input needs every transform start 16-byte
+// aligned: base address and distance (floats) a multiple of 4.
+static bool stage_ok(const float* x, long long dist) {
+    const char* env = std::getenv("FAF_CUDA_NO_STAGING");
+    if (env && env[0] == '1') return false;
+    return ((unsigned long long)(size_t)x % 16 == 0) && (dist % 4 == 0);
+}
+
+// FAF_CUDA_STAGING=1 turns input staging on for kernels that default to off.
+static bool stage_env() {
+    const char* env = std::getenv("FAF_CUDA_STAGING");
+    return env && env[0] == '1';
 }
 
 // ---------------------------------------------------------------------------
@@ -280,6 +305,7 @@ void plan_free(DevicePlan* p) {
     cudaFree(p->d_window);
     cudaFree(p->d_stage);
     cudaFree(p->d_scratch);
+    cudaFree(p->d_work);
     delete p;
 }
 
@@ -296,13 +322,73 @@ static bool is_7_smooth(long long n) {
     return n == 1;
 }
 
+// ---- four-step plans ------------------------------------------------------
+
+// Minimum threads of the runtime-radix engine for length m (16 values per
+// thread per stage), or a large number if m is not 7-smooth.
+static int min_threads(int m) {
+    std::vector<int> rad;
+    if (!radix_program(m, rad)) return 1 << 30;
+    int T = 1;
+    for (int R : rad) {
+        const int mb = std::max(1, kE / R);
+        T = std::max(T, ((m / R) + mb - 1) / mb);
+    }
+    return T;
+}
+
+// Threads per sub-transform, padded to a power of two dividing the CTA size
+// (so every thread of the CTA belongs to a group in both passes).
+static int padded_threads(int m) {
+    const int t = min_threads(m);
+    int p = 1;
+    while (p < t) p <<= 1;
+    return p;
+}
+
+// n = n1 * n2 with n1 <= n2, both 7-smooth and both within one group of a
+// kLargeThreads CTA; n1 the largest such divisor <= sqrt(n).
+static bool choose_factors(int n, int& n1, int& n2) {
+    n1 = n2 = 0;
+    for (int d = 2; (long long)d * d <= n; d++) {
+        if (n % d) continue;
+        const int e = n / d;
+        if (!is_7_smooth(d) || !is_7_smooth(e)) continue;
+        if (padded_threads(d) > fafk::kLargeThreads || padded_threads(e) > fafk::kLargeThreads)
+            continue;
+        n1 = d;
+        n2 = e;
+    }
+    return n1 > 0;
+}
+
+static bool build_large(DevicePlan* p, int n, std::string& err) {
+    if (!choose_factors(n, p->n1, p->n2)) {
+        err = "no four-step factorisation for length " + std::to_string(n);
+        return false;
+    }
+    if (!build_size(p->n1, p->f1, err) || !build_size(p->n2, p->f2, err)) return false;
+    p->t1 = padded_threads(p->n1);
+    p->t2 = padded_threads(p->n2);
+    std::vector<float2> w = twiddles(n);
+    if (!cuda_ok(upload(&p->d_tw_big, w.data(), w.size()), err, "twiddle upload")) return false;
+    p->large = true;
+    return true;
+}
+
+static bool is_prime(int n);
+static bool is_7_smooth(long long n);
+
 DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::string& err) {
     (void)flags;
     DevicePlan* p = nullptr;
     if (is_7_smooth(n)) {
         if (n > kMaxSingleCta) {
-            err = "C2C length " + std::to_string(n) + " needs the four-step path";
-            return nullptr;
+            p = new_plan(Kind::C2C_LARGE, n);
+            if (!build_large(p, n, err)) { plan_free(p); return nullptr; }
+            p->inverse = inverse;
+            p->scale = scale;
+            return p;
         }
         p = new_plan(Kind::C2C, n);
         if (!build_size(n, p->inner, err)) { plan_free(p); return nullptr; }
@@ -392,14 +478,11 @@ static bool upload_super_twiddles(DevicePlan* p, int nc, std::string& err) {
 
 DevicePlan* plan_r2c(int n, bool inverse, float scale, std::string& err) {
     const int nc = n / 2;
-    if (nc > kMaxSingleCta) {
-        err = "real length " + std::to_string(n) + " needs the four-step path";
-        return nullptr;
-    }
     DevicePlan* p = new_plan(inverse ? Kind::C2R : Kind::R2C, n);
     p->inverse = inverse;
     p->scale = scale;
-    if (!build_size(nc, p->inner, err) || !upload_super_twiddles(p, nc, err)) {
+    const bool ok = (nc > kMaxSingleCta) ? build_large(p, nc, err) : build_size(nc, p->inner, err);
+    if (!ok || !upload_super_twiddles(p, nc, err)) {
         plan_free(p);
         return nullptr;
     }
@@ -415,6 +498,10 @@ DevicePlan* plan_pipeline(int n, float scale_fwd, float scale_inv, std::string& 
 }
 
 DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err) {
+    if (n / 2 > kMaxSingleCta) {
+        err = "STFT frames longer than " + std::to_string(2 * kMaxSingleCta) + " samples";
+        return nullptr;
+    }
     DevicePlan* p = plan_r2c(n, false, scale, err);
     if (!p) return nullptr;
     p->kind = Kind::STFT;
@@ -437,10 +524,70 @@ DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err) {
 // Device-pointer execution
 // ---------------------------------------------------------------------------
 
+// ---- four-step execution ---------------------------------------------------
+
+static fafk::LargeArgs large_args(DevicePlan* p) {
+    fafk::LargeArgs a;
+    a.s1 = p->f1.shape(p->n1);
+    a.s1.T = p->t1;
+    a.s2 = p->f2.shape(p->n2);
+    a.s2.T = p->t2;
+    a.n1 = p->n1;
+    a.n2 = p->n2;
+    a.tw1 = p->f1.d_tw;
+    a.tw2 = p->f2.d_tw;
+    a.twn = p->d_tw_big;
+    a.scratch = nullptr;
+    a.cta_floats = 0;
+    return a;
+}
+
+// One CTA per SM keeps the per-CTA scratch (2 or 4 x n floats) L2-resident.
+static int large_grid(long long batch) {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    return (int)std::max(1LL, std::min<long long>(batch, sms));
+}
+
+static cudaError_t run_large(DevicePlan* p, int kind, const void* args, long long batch,
+                             cudaStream_t st) {
+    fafk::LargeArgs a = large_args(p);
+    const int grid = large_grid(batch);
+    a.cta_floats = (kind == 0 ? 2LL : 4LL) * p->n1 * p->n2;
+    const size_t bytes = (size_t)grid * (size_t)a.cta_floats * sizeof(float);
+    {
+        std::lock_guard<std::mutex> lk(p->mu);
+        if (p->work_bytes < bytes) {
+            cudaFree(p->d_work);
+            p->d_work = nullptr;
+            p->work_bytes = 0;
+            cudaError_t e = cudaMalloc(&p->d_work, bytes);
+            if (e != cudaSuccess) return e;
+            p->work_bytes = bytes;
+        }
+    }
+    a.scratch = (float*)p->d_work;
+    return fafk::launch_large(kind, a, args, batch, grid, st);
+}
+
 cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, float* out_re,
                      float* out_im, long long batch, long long in_dist, long long out_dist,
                      bool interleaved, const float* window, cudaStream_t st) {
     const float sgn = p->inverse ? -1.0f : 1.0f;
+    if (p->kind == Kind::C2C_LARGE) {
+        if (interleaved || window) return cudaErrorNotSupported;
+        fafk::C2CArgs a;
+        std::memset(&a, 0, sizeof a);
+        a.in_re = in_re; a.in_im = in_im; a.out_re = out_re; a.out_im = out_im;
+        a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
+        a.scale = p->scale; a.sgn = sgn;
+        return run_large(p, 0, &a, batch, st);
+    }
     if (p->kind == Kind::C2C) {
         fafk::C2CArgs a;
         a.in_re = in_re; a.in_im = in_im; a.out_re = out_re; a.out_im = out_im;
@@ -485,10 +632,14 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
     fafk::RealArgs a = real_args(p, batch);
     a.in_a = x; a.out_a = Xr; a.out_b = Xi;
     a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
+    if (p->large) {
+        if (a.interleaved) return cudaErrorNotSupported;
+        return run_large(p, 1, &a, batch, st);
+    }
     const int slots = p->inner.n + 1;
     if (p->inner.ct_log2)
         return fafk::launch_pot2(1, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch), st);
+                                 geometry_ct(p->inner, slots, batch, stage_ok(x, in_dist)), st);
     return fafk::launch_r2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);
 }
@@ -498,6 +649,10 @@ cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, 
     fafk::RealArgs a = real_args(p, batch);
     a.in_a = Xr; a.in_b = Xi; a.out_a = y;
     a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
+    if (p->large) {
+        if (a.interleaved) return cudaErrorNotSupported;
+        return run_large(p, 2, &a, batch, st);
+    }
     const int slots = p->inner.n + 1;
     if (p->inner.ct_log2)
         return fafk::launch_pot2(2, p->inner.ct_log2, p->inner.d_tws, &a,
@@ -515,10 +670,16 @@ cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long bat
     a.scale = p->scale * p->scale2;  // ops are linear: both norms fold into the store
     a.nops = std::min(nops, fafk::kMaxOps);
     for (int i = 0; i < a.nops; i++) a.ops[i] = ops[i];
+    if (p->large) {
+        if (a.interleaved) return cudaErrorNotSupported;
+        return run_large(p, 3, &a, batch, st);
+    }
     const int slots = p->inner.n + 1;
     if (p->inner.ct_log2)
+        // measured on B200 (n = 4096): the two-FFT pipeline runs best without
+        // input staging at ~256 threads per CTA
         return fafk::launch_pot2(3, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch), st);
+                                 geometry_ct(p->inner, slots, batch, stage_env(), 256), st);
     return fafk::launch_pipeline(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                                  p->inner.d_tw, a, st);
 }

@@ -40,7 +40,8 @@ bool build_size(int n, FftSize& out, std::string& err);
 void free_size(FftSize& s);
 int plane_floats(int slots);
 fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long batch);
-fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch);
+fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, bool staged = false,
+                           int target_threads = 512);
 
 enum class Kind {
     C2C,        // single-CTA C2C (5-smooth / codelet / 7-smooth inner sizes)
@@ -61,10 +62,13 @@ struct DevicePlan {
     float scale = 1.0f;    // norm scale of this transform
     float scale2 = 1.0f;   // pipeline: inverse-side scale
     FftSize inner;         // the FFT the kernels run
-    // four-step factors (C2C_LARGE)
+    // four-step path (inner complex length > kMaxSingleCta): n_inner = n1 * n2
+    bool large = false;
     FftSize f1, f2;
-    int n1 = 0, n2 = 0;
+    int n1 = 0, n2 = 0, t1 = 0, t2 = 0;  // padded thread counts per sub-transform
     float2* d_tw_big = nullptr;  // W_n^i for the four-step middle twiddles
+    void* d_work = nullptr;      // per-CTA four-step scratch, grown on first use
+    size_t work_bytes = 0;
     // tables
     float2* d_stw = nullptr;     // R2C super-twiddles
     float2* d_B = nullptr;       // Rader / Bluestein kernel spectrum

@@ -94,10 +94,10 @@ __device__ __forceinline__ float2* fast_ptr(const T& x) {
     else return x.s.d;
 }
 
-template <int N, int S, bool TWS_SMEM, class Src, class Snk>
+template <int N, int S, bool TWS_SMEM, class Src, class Snk, class Sync>
 __device__ __forceinline__ void ct_stage(float (&xr)[16], float (&xi)[16], int t,
                                          const float2* __restrict__ tws, const Src& src,
-                                         const Snk& snk) {
+                                         const Snk& snk, const Sync& sync) {
     using Pl = P2<N>;
     constexpr int R = Pl::radix(S), P = Pl::span(S), NB = N / R, T = Pl::T, MB = 16 / R;
     constexpr int LP = ilog2(P);
@@ -133,7 +133,7 @@ __device__ __forceinline__ void ct_stage(float (&xr)[16], float (&xi)[16], int t
         }
         Dft<R>::run(&xr[i * R], &xi[i * R]);
     }
-    if constexpr (Src::kSmem && Snk::kSmem) __syncthreads();
+    if constexpr (Src::kSmem && Snk::kSmem) sync();
 #pragma unroll
     for (int i = 0; i < MB; i++) {
         const int b = t + i * T;
@@ -157,43 +157,98 @@ __device__ __forceinline__ void ct_stage(float (&xr)[16], float (&xi)[16], int t
             }
         }
     }
-    if constexpr (Snk::kSmem) __syncthreads();
+    if constexpr (Snk::kSmem) sync();
 }
 
-template <int N, int S, bool TWS_SMEM, class Src, class Snk>
+// Barrier of one transform group: a named barrier over the group's T threads
+// when T >= 32 (groups of a CTA then progress independently), a warp barrier
+// when the group lives inside one warp.
+struct GroupSync {
+    int id;          // 1..15 (0 is the CTA-wide barrier)
+    int nthreads;    // T
+    unsigned lanes;  // T < 32: lanes of this warp that exist (a CTA may end mid-warp)
+    __device__ __forceinline__ void operator()() const {
+        if (nthreads >= 32)
+            asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(nthreads) : "memory");
+        else
+            __syncwarp(lanes);
+    }
+    __device__ static GroupSync make(int g, int T) {
+        const int base = threadIdx.x & ~31;
+        const int n = min(32, (int)blockDim.x - base);
+        return GroupSync{1 + g, T, n >= 32 ? 0xffffffffu : ((1u << n) - 1u)};
+    }
+};
+
+struct NoHook {
+    __device__ __forceinline__ void operator()() const {}
+};
+
+template <int N, int S, bool TWS_SMEM, class Src, class Snk, class Sync, class Hook>
 __device__ __forceinline__ void ct_run(float (&xr)[16], float (&xi)[16], int t, float2* ws,
                                        const float2* __restrict__ tws, const Src& src,
-                                       const Snk& snk) {
+                                       const Snk& snk, const Sync& sync, const Hook& hook) {
     using Pl = P2<N>;
     const SmemC mid{ws};
     const LastC<Snk> last{snk};
     if constexpr (Pl::NS == 1) {
         if constexpr (Src::kSmem) {
-            ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid);
+            ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid, sync);
+            hook();
             for (int i = t; i < N; i += Pl::T) last.put(i, mid.get(i));
         } else {
-            ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, last);
+            ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, last, sync);
+            sync();
+            hook();
         }
     } else if constexpr (S == 0) {
-        ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid);
-        ct_run<N, 1, TWS_SMEM>(xr, xi, t, ws, tws, mid, snk);
+        // stage 0 ends with a barrier: the source is no longer read by anyone
+        ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid, sync);
+        hook();
+        ct_run<N, 1, TWS_SMEM>(xr, xi, t, ws, tws, mid, snk, sync, NoHook());
     } else if constexpr (S == Pl::NS - 1) {
-        ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, last);
+        ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, last, sync);
     } else {
-        ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, mid);
-        ct_run<N, S + 1, TWS_SMEM>(xr, xi, t, ws, tws, mid, snk);
+        ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, mid, sync);
+        ct_run<N, S + 1, TWS_SMEM>(xr, xi, t, ws, tws, mid, snk, sync, NoHook());
     }
 }
 
 // Forward FFT of N points (compile time) by the T = N/16 threads of one
 // transform group; `ws` is the group's interleaved workspace, `tws` the
 // per-stage twiddle table (shared memory when TWS_SMEM, else global).
-template <int N, bool TWS_SMEM, class Src, class Snk>
+template <int N, bool TWS_SMEM, class Src, class Snk, class Sync, class Hook = NoHook>
 __device__ __forceinline__ void ct_fft(int t, float2* ws, const float2* __restrict__ tws,
-                                       const Src& src, const Snk& snk) {
+                                       const Src& src, const Snk& snk, const Sync& sync,
+                                       const Hook& hook = Hook()) {
     float xr[16], xi[16];
-    if constexpr (!Src::kSmem) __syncthreads();
-    ct_run<N, 0, TWS_SMEM>(xr, xi, t, ws, tws, src, snk);
+    if constexpr (!Src::kSmem) sync();
+    ct_run<N, 0, TWS_SMEM>(xr, xi, t, ws, tws, src, snk, sync, hook);
 }
+
+// ---- asynchronous input staging (cp.async, 16-byte chunks) ---------------
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Staged input in shared memory, linear (no padding).  It is a different
+// buffer from the workspace, so the first stage needs no read/write barrier
+// (kSmem = false); the barrier at the start of ct_fft publishes the copies.
+struct StageSrc {
+    const float2* s;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ cf get(int i) const {
+        const float2 v = s[i];
+        return cf{v.x, v.y};
+    }
+};
 
 }  // namespace fafct

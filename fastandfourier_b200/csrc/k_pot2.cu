@@ -21,19 +21,30 @@ using fafct::plane2;
 
 // Shared-memory layout of one CTA:
 //   [twiddle table, if it fits 32 KB] [group 0 workspace] [group 1 ...] ...
+// Every region is a whole number of 16-byte units (an even float2 count):
+// cp.async needs 16-byte aligned shared-memory destinations.
+__host__ __device__ constexpr int even2(int x) { return (x + 1) & ~1; }
+
 template <int N>
 struct CtCfg {
     static constexpr bool TW_SMEM = P2<N>::TW * 8 <= 32768;
-    static constexpr int TWN = TW_SMEM ? (P2<N>::TW > 0 ? P2<N>::TW : 1) : 0;
+    static constexpr int TWN = TW_SMEM ? even2(P2<N>::TW > 0 ? P2<N>::TW : 1) : 0;
 };
+
+// float2 units of one group: workspace (+ input staging)
+__host__ __device__ constexpr int group_stride(int n, int slots, bool staged) {
+    return even2(plane2(slots)) + (staged ? n : 0);
+}
 
 template <int N>
 struct CtGroup {
     int g, t;
     float2* ws;
+    float2* stage;  // per-group input staging (N float2), when the kernel stages
     const float2* tw;
-    // Every kernel body begins with a barrier, which publishes the table.
-    __device__ __forceinline__ CtGroup(float2* sm, int slots, const float2* __restrict__ gtw) {
+    fafct::GroupSync sync;
+    __device__ __forceinline__ CtGroup(float2* sm, int slots, const float2* __restrict__ gtw,
+                                       bool staged = false) {
         constexpr int T = P2<N>::T;
         g = threadIdx.x / T;
         t = threadIdx.x % T;
@@ -43,8 +54,34 @@ struct CtGroup {
         } else {
             tw = gtw;
         }
-        ws = sm + CtCfg<N>::TWN + (size_t)g * plane2(slots);
+        ws = sm + CtCfg<N>::TWN + (size_t)g * group_stride(N, slots, staged);
+        stage = ws + even2(plane2(slots));
+        sync = fafct::GroupSync::make(g, T);
+        // publish the twiddle table to the whole CTA once
+        if constexpr (CtCfg<N>::TW_SMEM) __syncthreads();
     }
+};
+
+// Prefetch of one real signal (2N floats, 16-byte aligned) into the group's
+// staging buffer: N/2 chunks of 16 bytes, 8 per thread.
+template <int N>
+__device__ __forceinline__ void prefetch_real(float2* stage, const float* x, int t, bool live) {
+    if (live) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int c = t + j * P2<N>::T;
+            fafct::cp_async16(stage + 2 * c, x + 4 * c);
+        }
+    }
+    fafct::cp_async_commit();
+}
+
+template <int N>
+struct PrefetchNext {
+    float2* stage;
+    const float* x;  // next signal's input, or NULL
+    int t;
+    __device__ __forceinline__ void operator()() const { prefetch_real<N>(stage, x, t, x != nullptr); }
 };
 
 template <int N>
@@ -70,7 +107,7 @@ __global__ void __launch_bounds__(1024) k2_c2c(const float2* __restrict__ tws, c
                      a.interleaved, live};
         SplitSink snk{a.out_re + oo, a.interleaved ? nullptr : a.out_im + oo, a.scale, a.sgn,
                       a.interleaved, live};
-        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, src, snk);  // begins with a barrier
+        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, src, snk, q.sync);  // begins with a barrier
     }
 }
 
@@ -94,19 +131,32 @@ __device__ __forceinline__ void ct_r2c_post(int t, const SmemC& mid,
     }
 }
 
-template <int N>
+template <int N, bool ASYNC>
 __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, const RealArgs a,
                                                int G, bool vec) {
     extern __shared__ float4 smem4[];
-    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws);
+    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws, ASYNC);
     const SmemC mid{q.ws};
     const int fpe = a.interleaved ? 2 : 1;
+    if constexpr (ASYNC) {
+        const long long b0 = (long long)blockIdx.x * G + q.g;
+        prefetch_real<N>(q.stage, a.in_a + b0 * a.in_dist, q.t, b0 < a.batch);
+    }
     CT_FOR_GROUPS(G, a.batch) {
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid);
-        __syncthreads();
+        if constexpr (ASYNC) {
+            const long long bn = (grp_ + gridDim.x) * G + q.g;
+            const float* xn = bn < a.batch ? a.in_a + bn * a.in_dist : nullptr;
+            fafct::cp_async_wait_all();
+            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{q.stage}, mid, q.sync,
+                              PrefetchNext<N>{q.stage, xn, q.t});
+        } else {
+            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
+                              mid, q.sync);
+        }
+        q.sync();
         if (live) {
             const long long oo = bi * a.out_dist * fpe;
             HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo, a.interleaved};
@@ -129,8 +179,8 @@ __global__ void __launch_bounds__(1024) k2_stft(const float2* __restrict__ tws, 
         const long long sig = bi / a.frames, f = bi - sig * a.frames;
         ct_fft<N, kTw<N>>(q.t, q.ws, q.tw,
                           FrameSrc{a.in_a + sig * a.sig_len + f * a.hop, a.window, a.win, live},
-                          mid);
-        __syncthreads();
+                          mid, q.sync);
+        q.sync();
         if (live) {
             const long long oo = bi * a.out_dist * fpe;
             HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo, a.interleaved};
@@ -152,7 +202,7 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
         const long long io = bi * a.in_dist * fpe;
-        __syncthreads();  // the previous transform's last stage may still read ws
+        q.sync();  // the previous transform's last stage may still read ws
         for (int k = q.t; k <= nc; k += T) {
             cf v{0.f, 0.f};
             if (live) {
@@ -165,7 +215,7 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
             }
             mid.put(k, v);
         }
-        __syncthreads();
+        q.sync();
         for (int k = q.t; k <= nc / 2; k += T) {
             if (k == 0) {
                 const cf x0 = mid.get(0), xn = mid.get(nc);
@@ -177,9 +227,9 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
                 mid.put(nc - k, Znk);
             }
         }
-        __syncthreads();
+        q.sync();
         ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
-                          RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec});
+                          RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec}, q.sync);
     }
 }
 
@@ -207,19 +257,32 @@ __device__ __forceinline__ cf apply_ops2(const RealArgs& a, int k, cf v) {
     return v;
 }
 
-template <int N>
+template <int N, bool ASYNC>
 __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ tws,
                                                     const RealArgs a, int G, bool vec) {
     extern __shared__ float4 smem4[];
     constexpr int nc = N, T = P2<N>::T;
-    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws);
+    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws, ASYNC);
     const SmemC mid{q.ws};
+    if constexpr (ASYNC) {
+        const long long b0 = (long long)blockIdx.x * G + q.g;
+        prefetch_real<N>(q.stage, a.in_a + b0 * a.in_dist, q.t, b0 < a.batch);
+    }
     CT_FOR_GROUPS(G, a.batch) {
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid);
-        __syncthreads();
+        if constexpr (ASYNC) {
+            const long long bn = (grp_ + gridDim.x) * G + q.g;
+            const float* xn = bn < a.batch ? a.in_a + bn * a.in_dist : nullptr;
+            fafct::cp_async_wait_all();
+            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{q.stage}, mid, q.sync,
+                              PrefetchNext<N>{q.stage, xn, q.t});
+        } else {
+            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
+                              mid, q.sync);
+        }
+        q.sync();
         // Per bin pair: post-pass -> ops -> pre-pass, in registers.
         for (int k = q.t; k <= nc / 2; k += T) {
             if (k == 0) {
@@ -240,9 +303,9 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
                 mid.put(nc - k, Znk);
             }
         }
-        __syncthreads();
+        q.sync();
         ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
-                          RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec});
+                          RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec}, q.sync);
     }
 }
 
@@ -288,9 +351,15 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     }
     case 1: {
         const RealArgs& a = *(const RealArgs*)args;
-        if ((e = prep(k2_r2c<N>, g.smem)) != cudaSuccess) return e;
-        k2_r2c<N><<<persistent_grid(k2_r2c<N>, g, a.batch), g.threads, g.smem, st>>>(
-            tws, a, g.G, vec_ok(a.in_a, a.in_dist));
+        if (g.staged) {
+            if ((e = prep(k2_r2c<N, true>, g.smem)) != cudaSuccess) return e;
+            k2_r2c<N, true><<<persistent_grid(k2_r2c<N, true>, g, a.batch), g.threads, g.smem,
+                              st>>>(tws, a, g.G, true);
+        } else {
+            if ((e = prep(k2_r2c<N, false>, g.smem)) != cudaSuccess) return e;
+            k2_r2c<N, false><<<persistent_grid(k2_r2c<N, false>, g, a.batch), g.threads, g.smem,
+                               st>>>(tws, a, g.G, vec_ok(a.in_a, a.in_dist));
+        }
         break;
     }
     case 2: {
@@ -302,9 +371,16 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     }
     case 3: {
         const RealArgs& a = *(const RealArgs*)args;
-        if ((e = prep(k2_pipeline<N>, g.smem)) != cudaSuccess) return e;
-        k2_pipeline<N><<<persistent_grid(k2_pipeline<N>, g, a.batch), g.threads, g.smem, st>>>(
-            tws, a, g.G, vec_ok(a.in_a, a.in_dist) && vec_ok(a.out_a, a.out_dist));
+        const bool vec = vec_ok(a.in_a, a.in_dist) && vec_ok(a.out_a, a.out_dist);
+        if (g.staged) {
+            if ((e = prep(k2_pipeline<N, true>, g.smem)) != cudaSuccess) return e;
+            k2_pipeline<N, true><<<persistent_grid(k2_pipeline<N, true>, g, a.batch), g.threads,
+                                   g.smem, st>>>(tws, a, g.G, vec);
+        } else {
+            if ((e = prep(k2_pipeline<N, false>, g.smem)) != cudaSuccess) return e;
+            k2_pipeline<N, false><<<persistent_grid(k2_pipeline<N, false>, g, a.batch),
+                                    g.threads, g.smem, st>>>(tws, a, g.G, vec);
+        }
         break;
     }
     case 4: {

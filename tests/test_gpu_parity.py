@@ -327,3 +327,45 @@ def test_generic_engine_power_of_two(cuda, n, monkeypatch):
     x = seeded(200 + n).standard_normal((3, 2 * n)).astype(np.float32)
     Xr, Xi = F.Transform.rfft(2 * n).r2c(dev(torch, x))
     assert orc.rel_l2_complex(host(Xr), host(Xi), orc.fp64_r2c(x)) <= REL_L2_TOL
+
+
+LARGE_C2C = [20000, 24576, 32768, 40000, 65536]
+
+
+@pytest.mark.parametrize("n", LARGE_C2C)
+@pytest.mark.parametrize("inverse", [False, True])
+def test_four_step_c2c(cuda, n, inverse):
+    """Transforms longer than one CTA: the four-step path through per-CTA scratch."""
+    import fastandfourier_b200 as F
+    t, e_orc, e_64 = _c2c_case(cuda, F, n, inverse, batch=2)
+    assert t.kind == "c2c-4step"
+    assert e_orc <= REL_L2_TOL and e_64 <= REL_L2_TOL, (n, e_orc, e_64)
+
+
+def test_four_step_persistent_batch(cuda):
+    """More transforms than resident CTAs: every CTA loops over several."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n, batch = 32768, 300
+    rng = seeded(77)
+    re = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    im = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    t = F.Transform.fft(n, norm=F.N_ORTHO)
+    yr, yi = t.c2c(dev(torch, re), dev(torch, im))
+    want = orc.fp64_c2c(re, im, norm=2)
+    assert orc.rel_l2_complex(host(yr), host(yi), want) <= REL_L2_TOL
+
+
+@pytest.mark.parametrize("n", [40000, 65536])
+def test_four_step_real(cuda, n):
+    import fastandfourier_b200 as F
+    torch = cuda
+    x = seeded(300 + n).standard_normal((3, n)).astype(np.float32)
+    fwd = F.Transform.rfft(n)
+    Xr, Xi = fwd.r2c(dev(torch, x))
+    assert orc.rel_l2_complex(host(Xr), host(Xi), orc.fp64_r2c(x)) <= REL_L2_TOL
+    y = host(fwd.inverse().c2r(Xr, Xi))
+    assert orc.rel_l2(y, x) <= REL_L2_TOL
+    p = F.Transform.chirp(f"(pipeline (rfft :size {n}) conj (bandpass :lo 5 :hi 9000) (irfft))")
+    yp = host(p.pipeline(dev(torch, x)))
+    assert orc.rel_l2(yp, orc.pipeline(x, [(1, 0, 0), (3, 5, 9000)])) <= REL_L2_TOL
