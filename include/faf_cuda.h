@@ -50,6 +50,24 @@ int faf_cuda_synchronize(const faf_transform *t);
 int faf_execute_batched(const faf_transform *t, faf_buffer *out, const faf_buffer *in,
                         size_t batch, size_t in_dist, size_t out_dist);
 
+/* ---- allocation-free four-step C2C ----------------------------------------- */
+
+/* No counterpart in the reference.  Runs `batch` packed C2C transforms of
+ * plan t (a C2C plan longer than 16384 points, i.e. the four-step path, up to
+ * 65536) on device buffers without allocating any memory.  It is meant for
+ * callers that must not allocate while they run: a real-time callback that
+ * cannot wait inside the driver's allocator, or a program whose device memory
+ * is fully reserved by another allocator so that a cudaMalloc would fail.
+ * The four-step scratch is a fixed 16 MiB array per GPU, held from the
+ * library's load until process exit; a length whose per-CTA scratch would
+ * exceed it, host buffers and other plan kinds are rejected with an error.
+ * All calls on a GPU share that array: launches that overlap on the GPU race
+ * and must be serialised by the caller.  The first call on each device looks
+ * up the array's device address and should come before any stream capture.
+ * Stream and synchronisation rules are those of faf_execute. */
+int faf_cuda_execute_c2c_noalloc(const faf_transform *t, float *out_re, float *out_im,
+                                 const float *in_re, const float *in_im, size_t batch);
+
 #ifdef __cplusplus
 }
 #endif
