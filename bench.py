@@ -63,7 +63,17 @@ WORKLOADS = {
                  16 * 16384, 5 * 16384 * 14),
     "stft": ("STFT Hann 1024 hop 256, 64 signals x 2^18 samples, seed 4", 1024, 64,
              None, None),
+    "uneven": ("uneven batch: 4096 C2C, lengths uniform over {12,17,31,60,240,1000,3072,6000,"
+               "16384,65536} (sorted by length), U[-1,1), seed 2, one persistent launch",
+               None, 4096, None, None),
 }
+
+UNEVEN_SET = [12, 17, 31, 60, 240, 1000, 3072, 6000, 16384, 65536]
+
+
+def uneven_lengths(batch=4096):
+    rng = np.random.default_rng(2)
+    return sorted(int(v) for v in rng.choice(UNEVEN_SET, batch))
 
 
 def make_inputs(workload, batch):
@@ -86,6 +96,11 @@ def make_inputs(workload, batch):
     if workload == "stft":
         rng = np.random.default_rng(4)
         return [rng.standard_normal((batch, 1 << 18), dtype=np.float32)]
+    if workload == "uneven":
+        total = sum(uneven_lengths(batch))
+        rng = np.random.default_rng(2)
+        return [rng.uniform(-1, 1, total).astype(np.float32),
+                rng.uniform(-1, 1, total).astype(np.float32)]
     raise ValueError(workload)
 
 
@@ -95,6 +110,8 @@ def stft_geometry(L, n=1024, win=1024, hop=256):
 
 
 def algorithmic_bytes(workload, batch):
+    if workload == "uneven":
+        return 16 * sum(uneven_lengths(batch))
     if workload == "stft":
         L = 1 << 18
         F, bins = stft_geometry(L)
@@ -199,10 +216,12 @@ def build_transform(F, workload, torch):
         return F.Transform.fft(n)
     if workload == "stft":
         return F.Transform.stft(1024, win=1024, hop=256)
+    if workload == "uneven":
+        return F.Uneven(uneven_lengths(WORKLOADS["uneven"][2]), measure=True)
     raise ValueError(workload)
 
 
-def run_step(F, t, workload, ins, outs):
+def run_step(F, t, workload, ins, outs, plain=False):
     if workload == "pipeline":
         t.pipeline(ins[0], out=outs[0])
     elif workload == "r2c":
@@ -211,13 +230,26 @@ def run_step(F, t, workload, ins, outs):
         t.c2c(ins[0], ins[1], out_re=outs[0], out_im=outs[1])
     elif workload == "stft":
         t.stft_frames(ins[0], out_re=outs[0], out_im=outs[1])
+    elif workload == "uneven":
+        if hasattr(ins[0], "data_ptr"):
+            t.execute(ins[0], ins[1], outs[0], outs[1], plain=plain)
+        else:
+            # the uneven API takes device buffers: copies inside the step
+            import torch
+            d = [torch.from_numpy(a).cuda(non_blocking=True) for a in ins]
+            o = [torch.empty_like(d[0]), torch.empty_like(d[1])]
+            t.execute(d[0], d[1], o[0], o[1], plain=plain)
+            outs[0][:] = o[0].cpu().numpy()
+            outs[1][:] = o[1].cpu().numpy()
 
 
 def alloc_outputs(workload, batch, like, torch):
     n = WORKLOADS[workload][1]
-    dev = like.device if hasattr(like, "device") else None
-    mk = (lambda shp: torch.empty(shp, dtype=torch.float32, device=dev)) if dev is not None \
-        else (lambda shp: torch.empty(shp, dtype=torch.float32, pin_memory=True).numpy())
+    # torch tensors -> device outputs; numpy inputs -> pinned host numpy outputs
+    if hasattr(like, "data_ptr"):
+        mk = lambda shp: torch.empty(shp, dtype=torch.float32, device=like.device)  # noqa: E731
+    else:
+        mk = lambda shp: torch.empty(shp, dtype=torch.float32, pin_memory=True).numpy()  # noqa: E731
     if workload == "pipeline":
         return [mk((batch, n))]
     if workload == "r2c":
@@ -227,6 +259,9 @@ def alloc_outputs(workload, batch, like, torch):
     if workload == "stft":
         F_, bins = stft_geometry(1 << 18)
         return [mk((batch, F_, 513)), mk((batch, F_, 513))]
+    if workload == "uneven":
+        total = sum(uneven_lengths(batch))
+        return [mk((total,)), mk((total,))]
 
 
 def run_ours(args, rank, world, local_rank):
@@ -274,6 +309,21 @@ def run_ours(args, rank, world, local_rank):
         ms = float(tt.item())
     ms_per_step = ms / args.steps
     value = world * nbytes / (ms_per_step * 1e-3) / 1e9
+    plain = None
+    if workload == "uneven":
+        # the plain GPU method on the same data: one batched launch per length
+        for _ in range(3):
+            run_step(F, t, workload, ins, outs, plain=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            run_step(F, t, workload, ins, outs, plain=True)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        pms = ev0.elapsed_time(ev1) / args.steps
+        plain = {"value": round(nbytes / (pms * 1e-3) / 1e9, 1), "ms_per_step": round(pms, 4),
+                 "launches_per_step": len(set(uneven_lengths(batch))),
+                 "speedup_of_persistent": round(pms / ms_per_step, 3)}
 
     # end to end through the public API with pinned host buffers
     host_pinned = [torch.from_numpy(a).pin_memory().numpy() for a in host_in]
@@ -302,8 +352,8 @@ def run_ours(args, rank, world, local_rank):
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": ncu_traffic(workload),
                 "algorithmic_bytes_per_launch": nbytes,
-                "kernel": {"pipeline": "k_pipeline", "r2c": "k_r2c", "stft": "k_stft"}.get(
-                    workload, "k_c2c")}
+                "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
+                           "uneven": "k_uneven"}.get(workload, "k2_c2c")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -338,6 +388,8 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": launches,
             "clocks": sampler.result(),
         }
+        if plain is not None:
+            line["plain_one_launch_per_length"] = plain
         print(json.dumps(line), flush=True)
     t.close()
     t_e2e.close()
@@ -370,7 +422,37 @@ def _ref_call(refimpl, workload, sample_inputs, threads):
         refimpl.c2c(sample_inputs[0], sample_inputs[1], threads=threads)
     elif workload == "stft":
         refimpl.stft(sample_inputs[0], 1024, 1024, 256, threads=threads)
+    elif workload == "uneven":
+        # sample_inputs: (re, im, lengths) ragged; one reference batch per length
+        re, im, lengths = sample_inputs
+        off = 0
+        i = 0
+        while i < len(lengths):
+            j = i
+            while j < len(lengths) and lengths[j] == lengths[i]:
+                j += 1
+            n, cnt = lengths[i], j - i
+            refimpl.c2c(re[off:off + n * cnt].reshape(cnt, n), im[off:off + n * cnt].reshape(cnt, n),
+                        threads=threads)
+            off += n * cnt
+            i = j
 
+
+
+def cpu_sample(workload, host_in, count):
+    """A bounded sample of `count` transforms of the workload for the CPU
+    reference: (inputs for _ref_call, algorithmic bytes, transforms)."""
+    if workload == "uneven":
+        lengths = uneven_lengths(len(uneven_lengths()))
+        stride = max(1, len(lengths) // max(1, count))
+        offs = np.concatenate([[0], np.cumsum(lengths)])
+        pick = list(range(0, len(lengths), stride))[:count]
+        sl = [lengths[i] for i in pick]
+        re = np.concatenate([host_in[0][offs[i]:offs[i + 1]] for i in pick])
+        im = np.concatenate([host_in[1][offs[i]:offs[i + 1]] for i in pick])
+        return (re, im, sl), 16 * sum(sl), len(sl)
+    count = min(count, host_in[0].shape[0])
+    return [a[:count] for a in host_in], algorithmic_bytes(workload, count), count
 
 def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
     """The reference library (oracle/_ref, built from its own sources) on the
@@ -383,11 +465,13 @@ def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
             return {"value": None, "unit": "GB/s", "cores": 0, "kind": "reference",
                     "sample": f"unavailable: {e}"}
     threads = threads or host_threads()
-    batch = host_in[0].shape[0]
-    sample_b = batch if workload != "stft" else max(1, min(batch, threads))
-    sample = [a[:sample_b] for a in host_in]
-    _ref_call(refimpl, workload, [a[:min(sample_b, threads)] for a in sample], threads)  # warm
-    nbytes = algorithmic_bytes(workload, sample_b)
+    want = WORKLOADS[workload][2]
+    if workload == "stft":
+        want = max(1, min(want, threads))
+    elif workload == "uneven":
+        want = 512
+    sample, nbytes, sample_b = cpu_sample(workload, host_in, want)
+    _ref_call(refimpl, workload, sample, threads)  # warm
     reps, t0 = 0, time.perf_counter()
     while True:
         _ref_call(refimpl, workload, sample, threads)
@@ -417,8 +501,10 @@ def run_reference(args, rank, world):
             print(json.dumps({"impl": "reference", "unavailable": f"reference library missing: {e}"}))
             return
     # each step: a bounded sample of the workload (all host threads)
-    sample_b = min(batch, max(threads * 8, 64)) if workload != "stft" else min(batch, threads)
-    sample = [a[:sample_b] for a in host_in]
+    want = min(batch, max(threads * 8, 64)) if workload != "stft" else min(batch, threads)
+    if workload == "uneven":
+        want = min(batch, max(threads * 4, 64))
+    sample, nbytes, sample_b = cpu_sample(workload, host_in, want)
     for _ in range(max(args.warmup, 1)):
         _ref_call(refimpl, workload, sample, threads)
     times = []
@@ -427,7 +513,6 @@ def run_reference(args, rank, world):
         _ref_call(refimpl, workload, sample, threads)
         times.append(time.perf_counter() - t0)
     s = statistics.median(times)
-    nbytes = algorithmic_bytes(workload, sample_b)
     gbs = nbytes / s / 1e9
     line = {
         "impl": "reference",

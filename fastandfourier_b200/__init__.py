@@ -19,7 +19,7 @@ from ._lib import (B_CUDA, DIR_FORWARD, DIR_INVERSE, FLAG_BLUESTEIN, FLAG_MEASUR
                    N_FORWARD, N_NONE, N_ORTHO, T_FFT, T_IFFT, T_IRFFT, T_PIPELINE, T_RFFT,
                    T_STFT)
 
-__all__ = ["FafError", "Transform", "config", "lib", "available", "B_CUDA", "DIR_FORWARD",
+__all__ = ["FafError", "Transform", "Uneven", "config", "lib", "available", "B_CUDA", "DIR_FORWARD",
            "DIR_INVERSE", "FLAG_BLUESTEIN", "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
            "L_INTERLEAVED", "L_REAL", "L_SPLIT", "N_DEFAULT", "N_FORWARD", "N_NONE", "N_ORTHO",
            "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
@@ -89,6 +89,45 @@ def _empty_like_batch(ref, shape):
         return torch.empty(shape, dtype=torch.float32, device=ref.device)
     import numpy as np
     return np.empty(shape, np.float32)
+
+
+class Uneven:
+    """faf_uneven: many C2C transforms of different lengths, one persistent
+    launch.  Ragged packed split planes (transform i at offset sum of the
+    previous lengths)."""
+
+    def __init__(self, lengths, *, inverse=False, norm=N_DEFAULT, measure=False):
+        self.lengths = [int(n) for n in lengths]
+        arr = (ctypes.c_size_t * len(self.lengths))(*self.lengths)
+        c = config(0, dir=DIR_INVERSE if inverse else DIR_FORWARD, norm=norm,
+                   flags=FLAG_MEASURE if measure else 0)
+        self._p = C.lib().faf_uneven_create(arr, len(self.lengths), ctypes.byref(c))
+        if not self._p:
+            raise FafError(C.error())
+
+    @property
+    def total(self):
+        return C.lib().faf_uneven_total(self._p)
+
+    def set_stream(self, stream):
+        h = getattr(stream, "cuda_stream", stream)
+        _check(C.lib().faf_uneven_set_stream(self._p, h or None))
+
+    def execute(self, re, im, out_re, out_im, plain=False):
+        f = C.lib().faf_uneven_execute_plain if plain else C.lib().faf_uneven_execute
+        _check(f(self._p, _ptr(out_re), _ptr(out_im), _ptr(re), _ptr(im)))
+        return out_re, out_im
+
+    def close(self):
+        if self._p:
+            C.lib().faf_uneven_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Transform:

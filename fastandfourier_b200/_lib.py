@@ -106,6 +106,13 @@ _SIGS = [
     ("faf_cuda_synchronize", ctypes.c_int, [TP]),
     ("faf_cuda_execute_c2c_noalloc", ctypes.c_int,
      [TP] + [ctypes.c_void_p] * 4 + [ctypes.c_size_t]),
+    ("faf_uneven_create", ctypes.c_void_p, [ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t,
+                                             ctypes.POINTER(faf_config)]),
+    ("faf_uneven_execute", ctypes.c_int, [ctypes.c_void_p] * 5),
+    ("faf_uneven_execute_plain", ctypes.c_int, [ctypes.c_void_p] * 5),
+    ("faf_uneven_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("faf_uneven_total", ctypes.c_size_t, [ctypes.c_void_p]),
+    ("faf_uneven_destroy", None, [ctypes.c_void_p]),
     ("chirp_compile", TP, [ctypes.c_char_p]),
     ("chirp_bind", ctypes.c_int, [TP, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_size_t]),

@@ -86,7 +86,7 @@ struct LargeArgs {
     int n1, n2;
     const float2* tw1;     // N1-point twiddles
     const float2* tw2;     // N2-point twiddles
-    const float2* twn;     // n-point twiddles (middle factors W_n^{n2 k1})
+    const float2* twn;     // middle twiddles, entry k1 * n2 + c = W_n^{c k1}
     float* scratch;        // per-CTA scratch, cta_floats each
     long long cta_floats;
 };

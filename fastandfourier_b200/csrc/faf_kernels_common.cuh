@@ -232,6 +232,58 @@ inline bool vec_ok(const void* p, long long dist) {
     return (((unsigned long long)(size_t)p) % 8 == 0) && (dist % 2 == 0);
 }
 
+// ---- Rader convolution pieces (reference src/faf_fft_rader.c:136-232) ----
+
+struct GatherSrc {
+    const float* re;
+    const float* im;
+    const int* idx;
+    float sgn;
+    bool live;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ cf get(int j) const {
+        if (!live) return cf{0.f, 0.f};
+        const int s = __ldg(idx + j);
+        return cf{__ldg(re + s), sgn * __ldg(im + s)};
+    }
+};
+
+// Last-stage sink: multiply by B in place; keep bin 0 (the sum of the
+// gathered samples) for the DC term.
+struct MulBSink {
+    float* re;
+    float* im;
+    const float2* B;
+    float* dc;  // 2 floats per group, or NULL
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ void put(int j, cf v) const {
+        if (dc && j == 0) { dc[0] = v.x; dc[1] = v.y; }
+        const float2 w = __ldg(&B[j]);
+        const int p = fafd::pad(j);
+        re[p] = v.x * w.x - v.y * w.y;
+        im[p] = fmaf(v.x, w.y, v.y * w.x);
+    }
+};
+
+struct ScatterSink {
+    float* re;
+    float* im;
+    const int* idx;
+    float x0r, x0i;   // x[0] (conjugated for inverse)
+    float inv_m;
+    float scale, sgn;
+    bool live;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ void put(int j, cf v) const {
+        if (!live) return;
+        const int d = __ldg(idx + j);
+        // v is conj(unscaled inverse FFT); undo, scale by 1/m, add x0
+        const float yr = x0r + v.x * inv_m, yi = x0i - v.y * inv_m;
+        re[d] = yr * scale;
+        im[d] = sgn * yi * scale;
+    }
+};
+
 // Spectral ops of the fused pipeline on bin k (reference src/chirp.c:421-471,
 // src/faf_core.c:150-166): CONJ negates im; MUL multiplies by the bound H with
 // real DC and last-bin products; BANDPASS zeroes bins outside [lo, hi].

@@ -339,7 +339,7 @@ static int min_threads(int m) {
 
 // Threads per sub-transform, padded to a power of two dividing the CTA size
 // (so every thread of the CTA belongs to a group in both passes).
-static int padded_threads(int m) {
+int padded_threads(int m) {
     const int t = min_threads(m);
     int p = 1;
     while (p < t) p <<= 1;
@@ -362,7 +362,7 @@ static bool choose_factors(int n, int& n1, int& n2) {
     return n1 > 0;
 }
 
-static bool build_large(DevicePlan* p, int n, std::string& err) {
+bool build_large(DevicePlan* p, int n, std::string& err) {
     if (!choose_factors(n, p->n1, p->n2)) {
         err = "no four-step factorisation for length " + std::to_string(n);
         return false;
@@ -370,7 +370,13 @@ static bool build_large(DevicePlan* p, int n, std::string& err) {
     if (!build_size(p->n1, p->f1, err) || !build_size(p->n2, p->f2, err)) return false;
     p->t1 = padded_threads(p->n1);
     p->t2 = padded_threads(p->n2);
-    std::vector<float2> w = twiddles(n);
+    // middle twiddles laid out like the pass-1 output: [k1 * n2 + c] = W_n^{c k1}
+    std::vector<float2> w((size_t)n);
+    for (int k1 = 0; k1 < p->n1; k1++)
+        for (int c = 0; c < p->n2; c++) {
+            const double a = -2.0 * M_PI * (double)((long long)c * k1) / (double)n;
+            w[(size_t)k1 * p->n2 + c] = make_float2((float)std::cos(a), (float)std::sin(a));
+        }
     if (!cuda_ok(upload(&p->d_tw_big, w.data(), w.size()), err, "twiddle upload")) return false;
     p->large = true;
     return true;

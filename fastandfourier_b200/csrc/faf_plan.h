@@ -66,7 +66,7 @@ struct DevicePlan {
     bool large = false;
     FftSize f1, f2;
     int n1 = 0, n2 = 0, t1 = 0, t2 = 0;  // padded thread counts per sub-transform
-    float2* d_tw_big = nullptr;  // W_n^i for the four-step middle twiddles
+    float2* d_tw_big = nullptr;  // four-step middle twiddles [k1 * n2 + c] = W_n^{c k1}
     void* d_work = nullptr;      // per-CTA four-step scratch, grown on first use
     size_t work_bytes = 0;
     // tables
@@ -107,6 +107,12 @@ cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long bat
                           int nops, cudaStream_t st);
 cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long long n_sig,
                       long long sig_len, long long frames, bool interleaved, cudaStream_t st);
+
+// Four-step tables of p for complex length n (n1, n2, f1, f2, t1, t2, twiddles).
+bool build_large(DevicePlan* p, int n, std::string& err);
+// Threads per sub-transform of the runtime-radix engine for length m, padded to
+// a power of two (so that groups tile a power-of-two CTA exactly).
+int padded_threads(int m);
 
 // Host FFT in double precision (table generation only).
 void host_dft_fp64(std::vector<double>& re, std::vector<double>& im);

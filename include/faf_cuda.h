@@ -6,6 +6,8 @@
  *
  *   - streams: faf_cuda_set_stream / faf_cuda_synchronize
  *   - batched execute: many transforms of one plan in one launch
+ *   - uneven batches: transforms of different lengths in one persistent,
+ *     CUDA-graph-captured launch (faf_uneven_*)
  *
  * Pointers are plain `void *` / `float *` so the header needs no CUDA
  * include; a `void *stream` is a cudaStream_t.
@@ -49,6 +51,28 @@ int faf_cuda_synchronize(const faf_transform *t);
  * out inside the call. */
 int faf_execute_batched(const faf_transform *t, faf_buffer *out, const faf_buffer *in,
                         size_t batch, size_t in_dist, size_t out_dist);
+
+/* ---- uneven batches (one persistent launch) ------------------------------- */
+
+typedef struct faf_uneven faf_uneven;
+
+/* Plan `count` C2C transforms of the given lengths, each a legal
+ * faf_create_fft size <= 65536 (5-smooth, codelet or Rader prime).  cfg gives
+ * dir / norm / flags (n is ignored); FAF_FLAG_MEASURE runs the launch-shape
+ * autotuner on the plan's own workload.  Layout: split planes, ragged and
+ * packed -- transform i starts at element offset sum_{j<i} lengths[j]. */
+faf_uneven *faf_uneven_create(const size_t *lengths, size_t count, const faf_config *cfg);
+/* All transforms in one persistent launch (CUDA-graph replay while the
+ * device pointers stay the same).  Device buffers; synchronous unless a
+ * stream was set. */
+int faf_uneven_execute(faf_uneven *u, float *out_re, float *out_im, const float *in_re,
+                       const float *in_im);
+/* Reference GPU method: one batched launch per run of equal lengths. */
+int faf_uneven_execute_plain(faf_uneven *u, float *out_re, float *out_im, const float *in_re,
+                             const float *in_im);
+int faf_uneven_set_stream(faf_uneven *u, void *stream);
+size_t faf_uneven_total(const faf_uneven *u); /* total complex elements */
+void faf_uneven_destroy(faf_uneven *u);
 
 /* ---- allocation-free four-step C2C ----------------------------------------- */
 

@@ -157,3 +157,10 @@ def test_names_and_version():
     assert L.faf_norm_name(F.N_ORTHO) == b"ortho"
     assert L.faf_transform_name(F.T_PIPELINE) == b"pipeline"
     assert L.faf_precision_size(3) == 4
+
+
+def test_uneven_rejects_illegal_lengths():
+    with pytest.raises(F.FafError, match="legal faf_create_fft size"):
+        F.Uneven([60, 23])
+    with pytest.raises(F.FafError, match="empty"):
+        F.Uneven([])
