@@ -10,7 +10,14 @@ once, each output sample written once: 8 bytes per sample) and its fraction
 of the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload pipeline|r2c|c2c1024|c2c16384|stft]
+                    [--workload pipeline|r2c|c2c1024|c2c16384|stft|uneven|serve]
+
+--workload serve replays a Poisson request trace (20k requests/s: 40% rfft
+of log-uniform sizes 256..65536 rounded to the recommended size, 30% the
+notch pipeline, 30% STFT of log-uniform 2^16..2^20 samples) through the
+continuous-batching server and reports p50 / p99 latency and throughput,
+next to the same trace served one request at a time (no merging, one
+stream).
 
 --impl reference times the reference library's own CPU path (compiled from
 its sources into oracle/_ref) on all host cores over a bounded sample of the
@@ -67,6 +74,11 @@ WORKLOADS = {
                "16384,65536} (sorted by length), U[-1,1), seed 2, one persistent launch",
                None, 4096, None, None),
 }
+
+WORKLOADS["serve"] = ("serving trace: 4000 requests, Poisson 20k req/s (seed 4); 40% rfft "
+                      "N log-uniform [256, 65536] -> recommended size, 30% notch pipeline "
+                      "4096, 30% STFT Hann 1024 hop 256 over L log-uniform [2^16, 2^20]; "
+                      "inputs N(0,1) generated on the device", None, 4000, None, None)
 
 UNEVEN_SET = [12, 17, 31, 60, 240, 1000, 3072, 6000, 16384, 65536]
 
@@ -234,13 +246,20 @@ def run_step(F, t, workload, ins, outs, plain=False):
         if hasattr(ins[0], "data_ptr"):
             t.execute(ins[0], ins[1], outs[0], outs[1], plain=plain)
         else:
-            # the uneven API takes device buffers: copies inside the step
+            # the uneven API takes device buffers: pinned host -> device copies
+            # into buffers kept across steps (so the captured graph replays),
+            # then device -> pinned host copies of both output planes
             import torch
-            d = [torch.from_numpy(a).cuda(non_blocking=True) for a in ins]
-            o = [torch.empty_like(d[0]), torch.empty_like(d[1])]
-            t.execute(d[0], d[1], o[0], o[1], plain=plain)
-            outs[0][:] = o[0].cpu().numpy()
-            outs[1][:] = o[1].cpu().numpy()
+            if getattr(t, "_stage", None) is None:
+                t._stage = [torch.empty(a.shape, dtype=torch.float32, device="cuda")
+                            for a in list(ins) + list(outs)]
+            d = t._stage
+            for dev, host in zip(d[:2], ins):
+                dev.copy_(torch.from_numpy(host), non_blocking=True)
+            t.execute(d[0], d[1], d[2], d[3], plain=plain)
+            for dev, host in zip(d[2:], outs):
+                torch.from_numpy(host).copy_(dev, non_blocking=True)
+            torch.cuda.current_stream().synchronize()
 
 
 def alloc_outputs(workload, batch, like, torch):
@@ -539,6 +558,138 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+
+# ---------------------------------------------------------------------------
+# serving trace (continuous batching)
+# ---------------------------------------------------------------------------
+
+def serve_trace(F, n_req=4000, rate=20000.0, seed=4):
+    """Request kinds, sizes and arrival times of the serving trace."""
+    from fastandfourier_b200 import _lib as C
+    rng = np.random.default_rng(seed)
+    kinds = rng.choice(3, n_req, p=[0.4, 0.3, 0.3])
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    sizes = []
+    for k in kinds:
+        if k == 0:
+            n = int(np.exp(rng.uniform(np.log(256), np.log(65536))))
+            sizes.append(int(C.lib().faf_get_recommended_size(C.T_RFFT, n)))
+        elif k == 1:
+            sizes.append(4096)
+        else:
+            sizes.append(int(np.exp(rng.uniform(np.log(1 << 16), np.log(1 << 20)))))
+    return kinds, sizes, arrivals
+
+
+def build_serve_requests(F, torch, kinds, sizes, seed=4):
+    """Device inputs (N(0,1) from a seeded device generator) and outputs."""
+    nin = sum(sizes)
+    nout = 0
+    for k, n in zip(kinds, sizes):
+        nout += 2 * (n // 2 + 1) if k == 0 else n if k == 1 else 2 * stft_geometry(n)[1]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    xin = torch.randn(nin, device="cuda", generator=g)
+    xout = torch.empty(nout, device="cuda")
+    m = torch.from_numpy(notch_mask(4096)).cuda()
+    z = torch.zeros_like(m)
+    h = (m, z, 2049)
+    reqs, algo = [], 0
+    io = oo = 0
+    pipe = "(pipeline (rfft :size 4096) (mul-spectrum) (irfft))"
+    for k, n in zip(kinds, sizes):
+        x = xin[io:io + n]
+        io += n
+        if k == 0:
+            nb = n // 2 + 1
+            o_re, o_im = xout[oo:oo + nb], xout[oo + nb:oo + 2 * nb]
+            oo += 2 * nb
+            reqs.append(F.Request(x, o_re, o_im, chirp=f"(rfft :size {n})"))
+            algo += 4 * n + 8 * nb
+        elif k == 1:
+            o = xout[oo:oo + n]
+            oo += n
+            reqs.append(F.Request(x, o, chirp=pipe, h=h))
+            algo += 8 * n
+        else:
+            bins = stft_geometry(n)[1]
+            o_re, o_im = xout[oo:oo + bins], xout[oo + bins:oo + 2 * bins]
+            oo += 2 * bins
+            reqs.append(F.Request(x, o_re, o_im, stft=(1024, 1024, 256)))
+            algo += 4 * n + 8 * bins
+    return reqs, algo, (xin, xout, m, z)
+
+
+def serve_once(F, reqs, arrivals, *, streams, max_merge, budget=16 << 30):
+    srv = F.Server(hbm_budget=budget, streams=streams, max_merge=max_merge)
+    seen = set()
+    for r in reqs:  # plans (device tables) created ahead of the trace
+        key = (r.struct.chirp, r.struct.stft_n)
+        if key not in seen:
+            seen.add(key)
+            srv.prepare(r)
+    srv.replay(reqs[:200], arrivals[:200] - arrivals[0])  # warm-up
+    srv.reset_stats()
+    lat = srv.replay(reqs, arrivals)
+    st = srv.stats()
+    srv.close()
+    return st, lat
+
+
+def run_serve(args, rank, world, local_rank):
+    import torch
+    import fastandfourier_b200 as F
+    torch.cuda.set_device(local_rank)
+    desc = WORKLOADS["serve"][0]
+    kinds, sizes, arrivals = serve_trace(F, WORKLOADS["serve"][2])
+    reqs, algo, keep = build_serve_requests(F, torch, kinds, sizes)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    with sampler:
+        st, lat = serve_once(F, reqs, arrivals, streams=8, max_merge=64)
+    plain, _ = serve_once(F, reqs, arrivals, streams=1, max_merge=1)
+
+    def summary(s):
+        return {"p50_ms": round(1e3 * s["p50_latency_s"], 3),
+                "p99_ms": round(1e3 * s["p99_latency_s"], 3),
+                "max_ms": round(1e3 * s["max_latency_s"], 3),
+                "requests_per_s": round(s["requests_per_s"], 1),
+                "GB_per_s": round(s["bytes_per_s"] / 1e9, 2),
+                "launch_batches": s["batches"], "merged_requests": s["merged_requests"],
+                "completed": s["completed"], "failed": s["failed"]}
+
+    lat = np.asarray(lat)
+    by_kind = {}
+    for k, name in enumerate(("rfft", "pipeline", "stft")):
+        v = lat[np.asarray(kinds) == k]
+        if v.size:
+            by_kind[name] = {"p50_ms": round(1e3 * float(np.percentile(v, 50)), 3),
+                             "p99_ms": round(1e3 * float(np.percentile(v, 99)), 3)}
+    if rank == 0:
+        line = {
+            "metric": "served GB/s at the trace's arrival rate",
+            "value": round(st["bytes_per_s"] / 1e9, 2),
+            "unit": "GB/s",
+            "n_gpus": world,
+            "steps": 1,
+            "warmup": 1,
+            "ms_per_step": round(1e3 * st["wall_s"], 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded device N(0,1), Poisson arrivals)",
+            "config": {"workload": desc, "requests": len(reqs), "algorithmic_bytes": algo,
+                       "streams": 8, "max_merge": 64, "hbm_budget_bytes": 16 << 30},
+            "latency": summary(st),
+            "latency_by_kind": by_kind,
+            "plain_one_request_at_a_time": summary(plain),
+            "arena_peak_bytes": st["arena_peak_bytes"],
+            "clocks": sampler.result(),
+        }
+        print(json.dumps(line), flush=True)
+    del keep
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -554,7 +705,14 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if "WORLD_SIZE" not in os.environ:
         world = 1
-    if args.impl == "reference":
+    if args.workload == "serve":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no "
+                                  "request loop; its CPU path is timed by the other workloads"}))
+            return
+        run_serve(args, rank, world, local_rank)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     else:
         run_ours(args, rank, world, local_rank)

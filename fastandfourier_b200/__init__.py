@@ -19,8 +19,8 @@ from ._lib import (B_CUDA, DIR_FORWARD, DIR_INVERSE, FLAG_BLUESTEIN, FLAG_MEASUR
                    N_FORWARD, N_NONE, N_ORTHO, T_FFT, T_IFFT, T_IRFFT, T_PIPELINE, T_RFFT,
                    T_STFT)
 
-__all__ = ["FafError", "Transform", "Uneven", "config", "lib", "available", "B_CUDA", "DIR_FORWARD",
-           "DIR_INVERSE", "FLAG_BLUESTEIN", "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
+__all__ = ["FafError", "Transform", "Uneven", "Server", "Request", "config", "lib", "available",
+           "B_CUDA", "DIR_FORWARD", "DIR_INVERSE", "FLAG_BLUESTEIN", "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
            "L_INTERLEAVED", "L_REAL", "L_SPLIT", "N_DEFAULT", "N_FORWARD", "N_NONE", "N_ORTHO",
            "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
 
@@ -89,6 +89,96 @@ def _empty_like_batch(ref, shape):
         return torch.empty(shape, dtype=torch.float32, device=ref.device)
     import numpy as np
     return np.empty(shape, np.float32)
+
+
+class Request:
+    """One faf_request of the serving loop.  `chirp` names a real transform or
+    pipeline; without it, stft=(n, win, hop) asks for a framed STFT.  Buffers
+    are torch tensors or numpy arrays (host or device); they must stay alive
+    until the request completes (the object keeps references)."""
+
+    def __init__(self, x, out_re, out_im=None, *, chirp=None, stft=None, h=None,
+                 stream_key=0):
+        r = C.faf_request()
+        self._chirp = chirp.encode() if chirp else None
+        r.chirp = self._chirp
+        if stft is not None:
+            r.stft_n, r.stft_win, r.stft_hop = (int(v) for v in stft)
+        if h is not None:
+            r.h_re, r.h_im, r.h_len = _ptr(h[0]), _ptr(h[1]), int(h[2])
+        n = x.numel() if hasattr(x, "numel") else x.size
+        r.in_, r.in_len = _ptr(x), int(n)
+        r.out_re, r.out_im = _ptr(out_re), _ptr(out_im)
+        r.stream_key = int(stream_key)
+        self.struct = r
+        self.keep = (x, out_re, out_im, h)
+
+
+class Server:
+    """faf_server: continuous-batching request loop on one GPU."""
+
+    def __init__(self, hbm_budget=0, streams=0, max_merge=0):
+        c = C.faf_server_config(int(hbm_budget), int(streams), int(max_merge))
+        self._p = C.lib().faf_server_create(ctypes.byref(c))
+        if not self._p:
+            raise FafError(C.error())
+        self._live = {}
+
+    def submit(self, req):
+        rid = C.lib().faf_server_submit(self._p, ctypes.byref(req.struct))
+        if rid < 0:
+            raise FafError(C.error())
+        self._live[rid] = req
+        return rid
+
+    def wait(self, rid):
+        """(latency seconds, frames) of request rid, once it has completed."""
+        lat, fr = ctypes.c_double(), ctypes.c_size_t()
+        rc = C.lib().faf_server_wait(self._p, rid, ctypes.byref(lat), ctypes.byref(fr))
+        self._live.pop(rid, None)
+        _check(rc)
+        return lat.value, fr.value
+
+    def drain(self):
+        _check(C.lib().faf_server_drain(self._p))
+
+    def prepare(self, req):
+        _check(C.lib().faf_server_prepare(self._p, ctypes.byref(req.struct)))
+
+    def stream_frames(self, key, win, hop, in_len):
+        return C.lib().faf_server_stream_frames(self._p, key, win, hop, in_len)
+
+    def close_stream(self, key):
+        _check(C.lib().faf_server_close_stream(self._p, key))
+
+    def replay(self, reqs, arrivals):
+        """Submit reqs at arrival times (seconds from now) from the library's
+        own client loop; returns the per-request latencies."""
+        n = len(reqs)
+        arr = (C.faf_request * n)(*[r.struct for r in reqs])
+        t = (ctypes.c_double * n)(*[float(a) for a in arrivals])
+        lat = (ctypes.c_double * n)()
+        _check(C.lib().faf_server_replay(self._p, arr, t, n, lat))
+        return list(lat)
+
+    def stats(self):
+        st = C.faf_server_stats()
+        _check(C.lib().faf_server_stats_get(self._p, ctypes.byref(st)))
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def reset_stats(self):
+        C.lib().faf_server_stats_reset(self._p)
+
+    def close(self):
+        if self._p:
+            C.lib().faf_server_destroy(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Uneven:

@@ -64,6 +64,30 @@ faf_transform._fields_ = [
     ("custom_gt", ctypes.c_void_p), ("custom_len_hg", ctypes.c_int),
     ("custom_len_syn", ctypes.c_int), ("device_plan", ctypes.c_void_p)]
 
+class faf_server_config(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("streams", ctypes.c_int),
+                ("max_merge", ctypes.c_int)]
+
+
+class faf_request(ctypes.Structure):
+    _fields_ = [("chirp", ctypes.c_char_p), ("stft_n", ctypes.c_size_t),
+                ("stft_win", ctypes.c_size_t), ("stft_hop", ctypes.c_size_t),
+                ("h_re", ctypes.c_void_p), ("h_im", ctypes.c_void_p), ("h_len", ctypes.c_size_t),
+                ("in_", ctypes.c_void_p), ("in_len", ctypes.c_size_t),
+                ("out_re", ctypes.c_void_p), ("out_im", ctypes.c_void_p),
+                ("stream_key", ctypes.c_ulonglong)]
+
+
+class faf_server_stats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_longlong), ("failed", ctypes.c_longlong),
+                ("batches", ctypes.c_longlong), ("merged_requests", ctypes.c_longlong),
+                ("p50_latency_s", ctypes.c_double), ("p99_latency_s", ctypes.c_double),
+                ("mean_latency_s", ctypes.c_double), ("max_latency_s", ctypes.c_double),
+                ("wall_s", ctypes.c_double), ("requests_per_s", ctypes.c_double),
+                ("bytes_per_s", ctypes.c_double), ("arena_bytes", ctypes.c_size_t),
+                ("arena_peak_bytes", ctypes.c_size_t)]
+
+
 TP = ctypes.POINTER(faf_transform)
 BP = ctypes.POINTER(faf_buffer)
 SPECTRAL_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_float),
@@ -113,6 +137,22 @@ _SIGS = [
     ("faf_uneven_set_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("faf_uneven_total", ctypes.c_size_t, [ctypes.c_void_p]),
     ("faf_uneven_destroy", None, [ctypes.c_void_p]),
+    ("faf_server_create", ctypes.c_void_p, [ctypes.POINTER(faf_server_config)]),
+    ("faf_server_submit", ctypes.c_longlong, [ctypes.c_void_p, ctypes.POINTER(faf_request)]),
+    ("faf_server_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_longlong,
+                                       ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_size_t)]),
+    ("faf_server_drain", ctypes.c_int, [ctypes.c_void_p]),
+    ("faf_server_stream_frames", ctypes.c_size_t, [ctypes.c_void_p, ctypes.c_ulonglong]
+     + [ctypes.c_size_t] * 3),
+    ("faf_server_close_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.c_ulonglong]),
+    ("faf_server_prepare", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(faf_request)]),
+    ("faf_server_stats_get", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(faf_server_stats)]),
+    ("faf_server_stats_reset", None, [ctypes.c_void_p]),
+    ("faf_server_replay", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(faf_request),
+                                         ctypes.POINTER(ctypes.c_double), ctypes.c_size_t,
+                                         ctypes.POINTER(ctypes.c_double)]),
+    ("faf_server_destroy", None, [ctypes.c_void_p]),
     ("chirp_compile", TP, [ctypes.c_char_p]),
     ("chirp_bind", ctypes.c_int, [TP, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_size_t]),

@@ -346,6 +346,11 @@ int padded_threads(int m) {
     return p;
 }
 
+// Lengths that the single-CTA kernels cannot hold: above kMaxSingleCta, or
+// needing more than 1024 threads at 16 values per thread (e.g. 5^6 = 15625,
+// whose radix-5 stages keep 15 values per thread).  They take the four-step.
+bool needs_four_step(int n) { return n > kMaxSingleCta || min_threads(n) > 1024; }
+
 // n = n1 * n2 with n1 <= n2, both 7-smooth and both within one group of a
 // kLargeThreads CTA; n1 the largest such divisor <= sqrt(n).
 static bool choose_factors(int n, int& n1, int& n2) {
@@ -389,7 +394,7 @@ DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::stri
     (void)flags;
     DevicePlan* p = nullptr;
     if (is_7_smooth(n)) {
-        if (n > kMaxSingleCta) {
+        if (needs_four_step(n)) {
             p = new_plan(Kind::C2C_LARGE, n);
             if (!build_large(p, n, err)) { plan_free(p); return nullptr; }
             p->inverse = inverse;
@@ -487,7 +492,7 @@ DevicePlan* plan_r2c(int n, bool inverse, float scale, std::string& err) {
     DevicePlan* p = new_plan(inverse ? Kind::C2R : Kind::R2C, n);
     p->inverse = inverse;
     p->scale = scale;
-    const bool ok = (nc > kMaxSingleCta) ? build_large(p, nc, err) : build_size(nc, p->inner, err);
+    const bool ok = needs_four_step(nc) ? build_large(p, nc, err) : build_size(nc, p->inner, err);
     if (!ok || !upload_super_twiddles(p, nc, err)) {
         plan_free(p);
         return nullptr;
@@ -504,8 +509,8 @@ DevicePlan* plan_pipeline(int n, float scale_fwd, float scale_inv, std::string& 
 }
 
 DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err) {
-    if (n / 2 > kMaxSingleCta) {
-        err = "STFT frames longer than " + std::to_string(2 * kMaxSingleCta) + " samples";
+    if (needs_four_step(n / 2)) {
+        err = "STFT frames of " + std::to_string(n) + " samples exceed one CTA";
         return nullptr;
     }
     DevicePlan* p = plan_r2c(n, false, scale, err);

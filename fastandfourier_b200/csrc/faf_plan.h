@@ -113,6 +113,7 @@ bool build_large(DevicePlan* p, int n, std::string& err);
 // Threads per sub-transform of the runtime-radix engine for length m, padded to
 // a power of two (so that groups tile a power-of-two CTA exactly).
 int padded_threads(int m);
+bool needs_four_step(int n);
 
 // Host FFT in double precision (table generation only).
 void host_dft_fp64(std::vector<double>& re, std::vector<double>& im);

@@ -329,7 +329,10 @@ def test_generic_engine_power_of_two(cuda, n, monkeypatch):
     assert orc.rel_l2_complex(host(Xr), host(Xi), orc.fp64_r2c(x)) <= REL_L2_TOL
 
 
-LARGE_C2C = [20000, 24576, 32768, 40000, 65536]
+# 15552 / 15625 / 16000 fit the single-CTA length limit but need more than
+# 1024 threads at 16 values per thread (radix-3 / radix-5 stages), so they
+# take the four-step path too.
+LARGE_C2C = [15552, 15625, 16000, 20000, 24576, 32768, 40000, 65536]
 
 
 @pytest.mark.parametrize("n", LARGE_C2C)
@@ -356,7 +359,7 @@ def test_four_step_persistent_batch(cuda):
     assert orc.rel_l2_complex(host(yr), host(yi), want) <= REL_L2_TOL
 
 
-@pytest.mark.parametrize("n", [40000, 65536])
+@pytest.mark.parametrize("n", [31250, 32000, 40000, 65536])
 def test_four_step_real(cuda, n):
     import fastandfourier_b200 as F
     torch = cuda
