@@ -15,12 +15,13 @@ import ctypes
 
 from . import _lib as C
 from ._lib import (B_CUDA, DIR_FORWARD, DIR_INVERSE, FLAG_BLUESTEIN, FLAG_MEASURE,
+                   FLAG_TENSOR_CORE,
                    L_DEFAULT, L_HERMITIAN, L_INTERLEAVED, L_REAL, L_SPLIT, N_DEFAULT,
                    N_FORWARD, N_NONE, N_ORTHO, T_FFT, T_IFFT, T_IRFFT, T_PIPELINE, T_RFFT,
                    T_STFT)
 
 __all__ = ["FafError", "Transform", "Uneven", "Server", "Request", "config", "lib", "available",
-           "B_CUDA", "DIR_FORWARD", "DIR_INVERSE", "FLAG_BLUESTEIN", "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
+           "B_CUDA", "DIR_FORWARD", "DIR_INVERSE", "FLAG_TENSOR_CORE", "FLAG_BLUESTEIN", "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
            "L_INTERLEAVED", "L_REAL", "L_SPLIT", "N_DEFAULT", "N_FORWARD", "N_NONE", "N_ORTHO",
            "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
 
@@ -291,6 +292,11 @@ class Transform:
 
     def synchronize(self):
         _check(C.lib().faf_cuda_synchronize(self._p))
+
+    def tc_status(self):
+        """Tensor-core plans: 0 = every MMA wait completed, 1 = one ran out of
+        its bound; -1 for other plans."""
+        return C.lib().faf_cuda_tc_status(self._p)
 
     # ---- execute ----
     def execute(self, out, inp):

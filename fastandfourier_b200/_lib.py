@@ -24,6 +24,7 @@ DIR_FORWARD, DIR_INVERSE = 0, 1
 B_AUTO, B_VM, B_JIT, B_CUDA = 0, 1, 2, 3
 FLAG_INVERSE, FLAG_REAL = 0x1, 0x8
 FLAG_BLUESTEIN, FLAG_MEASURE = 1 << 12, 1 << 13
+FLAG_TENSOR_CORE = 1 << 16
 CHIRP_OP_CONJ, CHIRP_OP_MUL, CHIRP_OP_BANDPASS = 0x7FFFFFFD, 0x7FFFFFFE, 0x7FFFFFFF
 FAF_CALL_BUILTIN = 30
 
@@ -125,6 +126,7 @@ _SIGS = [
     ("faf_cuda_available", ctypes.c_int, []),
     ("faf_cuda_plan_kind", ctypes.c_char_p, [TP]),
     ("faf_cuda_last_launches", ctypes.c_int, []),
+    ("faf_cuda_tc_status", ctypes.c_int, [TP]),
     ("faf_cuda_set_stream", ctypes.c_int, [TP, ctypes.c_void_p]),
     ("faf_cuda_get_stream", ctypes.c_void_p, [TP]),
     ("faf_cuda_synchronize", ctypes.c_int, [TP]),

@@ -440,11 +440,21 @@ extern "C" int faf_cuda_available(void) {
     return 1;
 }
 
+extern "C" int faf_cuda_tc_status(const faf_transform* t) {
+    DevicePlan* p = plan_of(t);
+    if (!p || !p->tc) return -1;
+    int v = 0;
+    cudaError_t e = cudaStreamSynchronize(p->stream);
+    if (e == cudaSuccess) e = cudaMemcpy(&v, p->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "faf_cuda_tc_status");
+    return v ? 1 : 0;
+}
+
 extern "C" const char* faf_cuda_plan_kind(const faf_transform* t) {
     DevicePlan* p = plan_of(t);
     if (!p) return nullptr;
     switch (p->kind) {
-    case Kind::C2C: return "c2c";
+    case Kind::C2C: return p->tc ? "c2c-tc" : "c2c";
     case Kind::C2C_LARGE: return "c2c-4step";
     case Kind::RADER: return "rader";
     case Kind::BLUESTEIN: return "bluestein";

@@ -119,4 +119,9 @@ cudaError_t launch_pot2(int kind, int log2n, const float2* tws, const void* args
 // Shared-memory bytes the twiddle table of a log2n kernel adds to each CTA.
 size_t pot2_table_smem(int log2n);
 
+// Tensor-core precision form of the power-of-two C2C (k_tc.cu).
+bool tc_supported(int log2n);
+cudaError_t launch_c2c_tc(int log2n, const float2* tws, const C2CArgs& a, const void* gB,
+                          int* err, cudaStream_t st);
+
 }  // namespace fafk

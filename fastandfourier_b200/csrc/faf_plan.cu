@@ -2,6 +2,10 @@
 // device-pointer execution for every plan kind.
 #include "faf_plan.h"
 
+#include <cuda_fp16.h>
+
+#include "faf_cuda.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -303,6 +307,8 @@ void plan_free(DevicePlan* p) {
     cudaFree(p->d_rin);
     cudaFree(p->d_rout);
     cudaFree(p->d_window);
+    cudaFree(p->d_tcB);
+    cudaFree(p->d_tc_err);
     cudaFree(p->d_stage);
     cudaFree(p->d_scratch);
     cudaFree(p->d_work);
@@ -390,8 +396,41 @@ bool build_large(DevicePlan* p, int n, std::string& err) {
 static bool is_prime(int n);
 static bool is_7_smooth(long long n);
 
+// B operand of the tensor-core radix-16 stage: D = A B^T with A rows
+// (x_re[0..15], x_im[0..15]) and D rows (y_re[0..15], y_im[0..15]), so
+//   B[j][m] = Fr[j][m], B[j][16+m] = -Fi[j][m], B[16+j][m] = Fi[j][m],
+//   B[16+j][16+m] = Fr[j][m],   F[j][m] = exp(-2 pi i j m / 16) (FP64),
+// split into FP16 hi = fp16(B) and lo = fp16(B - hi), each stored K-major
+// without swizzle: element (n, k) at half index
+//   ((n % 8) * 16 + (n / 8) * 128 + (k / 8) * 512 + (k % 8) * 2) / 2.
+static bool build_tc_tables(DevicePlan* p, std::string& err) {
+    std::vector<uint16_t> h(2 * 1024, 0);
+    for (int n = 0; n < 32; n++)
+        for (int k = 0; k < 32; k++) {
+            const int j = n & 15, m = k & 15;
+            const double a = -2.0 * M_PI * (double)((j * m) % 16) / 16.0;
+            const double fr = std::cos(a), fi = std::sin(a);
+            double v;
+            if (n < 16) v = k < 16 ? fr : -fi;
+            else v = k < 16 ? fi : fr;
+            const __half hi = __double2half(v);
+            const __half lo = __double2half(v - (double)__half2float(hi));
+            const size_t idx = ((size_t)(n % 8) * 16 + (size_t)(n / 8) * 128 +
+                                (size_t)(k / 8) * 512 + (size_t)(k % 8) * 2) / 2;
+            h[idx] = __half_as_ushort(hi);
+            h[1024 + idx] = __half_as_ushort(lo);
+        }
+    if (!cuda_ok(cudaMalloc(&p->d_tcB, h.size() * sizeof(uint16_t)), err, "tensor-core table") ||
+        !cuda_ok(cudaMemcpy(p->d_tcB, h.data(), h.size() * sizeof(uint16_t),
+                            cudaMemcpyHostToDevice), err, "tensor-core table") ||
+        !cuda_ok(cudaMalloc(&p->d_tc_err, sizeof(int)), err, "tensor-core flag") ||
+        !cuda_ok(cudaMemset(p->d_tc_err, 0, sizeof(int)), err, "tensor-core flag"))
+        return false;
+    p->tc = true;
+    return true;
+}
+
 DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::string& err) {
-    (void)flags;
     DevicePlan* p = nullptr;
     if (is_7_smooth(n)) {
         if (needs_four_step(n)) {
@@ -403,6 +442,11 @@ DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::stri
         }
         p = new_plan(Kind::C2C, n);
         if (!build_size(n, p->inner, err)) { plan_free(p); return nullptr; }
+        if ((flags & FAF_FLAG_TENSOR_CORE) && p->inner.ct_log2 &&
+            fafk::tc_supported(p->inner.ct_log2) && !build_tc_tables(p, err)) {
+            plan_free(p);
+            return nullptr;
+        }
     } else if (is_prime(n) && is_7_smooth(n - 1)) {
         // Rader: y = x0 + IDFT_m(DFT_m(x[g^j]) * DFT_m(W_p^{g^-j}))[...]
         const int m = n - 1;
@@ -606,6 +650,9 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         a.scale = p->scale; a.sgn = sgn; a.interleaved = interleaved ? 1 : 0;
         a.window = window;
         const int slots = p->inner.n;
+        if (p->tc)
+            return fafk::launch_c2c_tc(p->inner.ct_log2, p->inner.d_tws, a, p->d_tcB,
+                                       p->d_tc_err, st);
         if (p->inner.ct_log2)
             return fafk::launch_pot2(0, p->inner.ct_log2, p->inner.d_tws, &a,
                                      geometry_ct(p->inner, slots, batch), st);

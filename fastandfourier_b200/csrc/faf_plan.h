@@ -76,6 +76,11 @@ struct DevicePlan {
     int* d_rin = nullptr;        // Rader gather
     int* d_rout = nullptr;       // Rader scatter
     float* d_window = nullptr;   // STFT window
+    // tensor-core form (C2C, power of two): B = 16-point DFT as a 32 x 32
+    // real FP16 matrix, hi then lo, in the MMA's shared-memory layout
+    bool tc = false;
+    void* d_tcB = nullptr;
+    int* d_tc_err = nullptr;     // set by a kernel whose MMA wait ran out
     int win = 0, hop = 0;
     // launch state
     cudaStream_t stream = nullptr;  // 0 = legacy default stream

@@ -1,0 +1,65 @@
+// faf_pot2_group.cuh -- per-CTA shared-memory layout of the compile-time
+// power-of-two kernels (k_pot2.cu, k_tc.cu): twiddle table, then one
+// workspace per transform group.
+#pragma once
+
+#include "faf_kernels_common.cuh"
+#include "faf_pot2.cuh"
+
+namespace fafk {
+
+using fafct::P2;
+using fafct::plane2;
+
+// Shared-memory layout of one CTA:
+//   [twiddle table, if it fits 32 KB] [group 0 workspace] [group 1 ...] ...
+// Every region is a whole number of 16-byte units (an even float2 count):
+// cp.async needs 16-byte aligned shared-memory destinations.
+__host__ __device__ constexpr int even2(int x) { return (x + 1) & ~1; }
+
+template <int N>
+struct CtCfg {
+    static constexpr bool TW_SMEM = P2<N>::TW * 8 <= 32768;
+    static constexpr int TWN = TW_SMEM ? even2(P2<N>::TW > 0 ? P2<N>::TW : 1) : 0;
+};
+
+// float2 units of one group: workspace (+ input staging)
+__host__ __device__ constexpr int group_stride(int n, int slots, bool staged) {
+    return even2(plane2(slots)) + (staged ? n : 0);
+}
+
+template <int N>
+struct CtGroup {
+    int g, t;
+    float2* ws;
+    float2* stage;  // per-group input staging (N float2), when the kernel stages
+    const float2* tw;
+    fafct::GroupSync sync;
+    __device__ __forceinline__ CtGroup(float2* sm, int slots, const float2* __restrict__ gtw,
+                                       bool staged = false) {
+        constexpr int T = P2<N>::T;
+        g = threadIdx.x / T;
+        t = threadIdx.x % T;
+        if constexpr (CtCfg<N>::TW_SMEM) {
+            for (int i = threadIdx.x; i < CtCfg<N>::TWN; i += blockDim.x) sm[i] = __ldg(&gtw[i]);
+            tw = sm;
+        } else {
+            tw = gtw;
+        }
+        ws = sm + CtCfg<N>::TWN + (size_t)g * group_stride(N, slots, staged);
+        stage = ws + even2(plane2(slots));
+        sync = fafct::GroupSync::make(g, T);
+        // publish the twiddle table to the whole CTA once
+        if constexpr (CtCfg<N>::TW_SMEM) __syncthreads();
+    }
+};
+
+template <int N>
+constexpr bool kTw = CtCfg<N>::TW_SMEM;
+
+// Persistent loop over transform groups; uniform across the CTA.
+#define CT_FOR_GROUPS(G, batch)                                                          \
+    for (long long grp_ = blockIdx.x, ngrp_ = ((batch) + (G)-1) / (G); grp_ < ngrp_;     \
+         grp_ += gridDim.x)
+
+}  // namespace fafk

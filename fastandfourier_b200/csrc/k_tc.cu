@@ -1,0 +1,413 @@
+// k_tc.cu -- tensor-core precision form of the power-of-two C2C: every
+// radix-16 stage runs as tcgen05 MMAs, the remaining radix-8/4/2 stage on the
+// CUDA cores, in the compile-time Stockham engine of faf_pot2.cuh.
+//
+// One radix-16 stage of 128 butterflies (one warpgroup, one thread per
+// butterfly) is the real product
+//     D[128 x 32] = A[128 x 32] * B^T,   B[32 x 32] = [ Fr  -Fi ]
+//                                                   [ Fi   Fr ]
+// with A row = (x_re[0..15], x_im[0..15]) after the stage's twiddles and
+// D row = (y_re[0..15], y_im[0..15]), F = the 16-point forward DFT matrix.
+//
+// Precision: A and B are FP16, each split into hi + lo (hi = fp16(v), lo =
+// fp16(v - hi)), and D accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi in FP32
+// (six MMAs of K = 16).  The dropped A_lo B_lo term and the split residuals
+// are ~2^-22 of each operand, so a stage keeps FP32-level accuracy.  FP16's
+// range is handled per row: each thread scales its 32 values by a power of
+// two that puts the largest in [2^13, 2^14), and unscales D exactly.
+//
+// Operands: A tiles (hi, lo; 8 KB each per warpgroup, 128 KB for the CTA)
+// alias the Stockham workspace between the stage's reads and writes; B (hi,
+// lo) is a 4 KB constant built on the host from FP64 and copied to shared
+// memory once per CTA.  Both are K-major, no swizzle: element (row r, k) at
+// byte (r % 8) * 16 + (r / 8) * 128 + (k / 8) * LBO + (k % 8) * 2.
+// Accumulators: 128 TMEM lanes x 32 columns per warpgroup (256 columns per
+// CTA, one CTA per SM).  One thread per warpgroup issues the MMAs and commits
+// them to the warpgroup's mbarrier; the warpgroup waits on it (bounded: on
+// timeout the kernel records an error flag and finishes without hanging)
+// and reads its rows back with tcgen05.ld.
+#include <cuda_fp16.h>
+
+#include <algorithm>
+
+#include "faf_kernels_common.cuh"
+#include "faf_pot2.cuh"
+#include "faf_pot2_group.cuh"
+
+namespace fafk {
+namespace tc {
+
+using fafct::cf;
+using fafct::LastC;
+using fafct::SmemC;
+
+constexpr int kThreads = 1024;
+constexpr int kWarpgroups = kThreads / 128;
+constexpr uint32_t kTileBytes = 128 * 32 * 2;  // one FP16 A tile (128 rows x K 32)
+constexpr uint32_t kALbo = 16 * 128;           // A: K-direction core-matrix stride
+constexpr uint32_t kBLbo = 4 * 128;            // B: K-direction core-matrix stride
+constexpr uint32_t kSbo = 128;                 // both: next 8-row group
+constexpr uint32_t kBBytes = 2 * 32 * 32 * 2;  // B hi + lo
+constexpr uint32_t kTmemCols = 32 * kWarpgroups;
+// instruction descriptor (kind::f16): D F32 (bits 4-5 = 1), A and B F16
+// (bits 7-12 = 0), both K-major (bits 15-16 = 0), N >> 3 at bit 17, M >> 4 at 24
+constexpr uint32_t kIdesc = (1u << 4) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr int kSpinLimit = 1 << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor: start address, leading / stride byte
+// offsets (16-byte units), version 1 (bit 46), no swizzle.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ bool try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait; false when the limit ran out.
+__device__ __forceinline__ bool wait_bounded(uint64_t* bar, uint32_t parity) {
+    for (int i = 0; i < kSpinLimit; i++)
+        if (try_wait(bar, parity)) return true;
+    return false;
+}
+
+// 32 consecutive accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
+          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
+          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
+          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
+          "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// hi / lo FP16 pair of v (v already scaled into FP16 range)
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+    const __half2 h = __floats2half2_rn(a, b);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+struct Ctx {
+    uint32_t tmem;      // this warpgroup's accumulator columns, lane 0
+    uint32_t tmem_ld;   // this warp's lane quarter of them
+    uint32_t a_hi;      // shared address of this warpgroup's A hi tile (lo follows)
+    uint32_t b_hi;      // shared address of B hi (lo follows at +2048)
+    uint64_t* bar;      // this warpgroup's mbarrier
+    uint32_t phase;
+    int row;            // this thread's row in the tile
+    int* err;
+    bool leader;        // issues the warpgroup's MMAs
+};
+
+struct CtaSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+// Radix-16 stage S of the N-point transform on the tensor cores (one
+// butterfly per thread; same data movement as fafct::ct_stage).
+template <int N, int S, bool TWS_SMEM, class Src, class Snk>
+__device__ __forceinline__ void tc_stage(float (&xr)[16], float (&xi)[16], int t,
+                                         const float2* __restrict__ tws, const Src& src,
+                                         const Snk& snk, Ctx& c) {
+    using Pl = P2<N>;
+    static_assert(Pl::radix(S) == 16, "tensor-core stages are radix 16");
+    constexpr int P = Pl::span(S), NB = N / 16, LP = fafct::ilog2(P);
+    constexpr int OFF = Pl::tw_offset(S);
+    const int b = t;
+    // ---- inputs and the stage's twiddles (FP32)
+    if constexpr (fafct::is_fast<Src>::value && NB % 16 == 0) {
+        const float2* p = fafct::fast_ptr(src) + fafct::pad2(b);
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            const float2 v = p[r * (NB + NB / 16)];
+            xr[r] = v.x;
+            xi[r] = Src::kConj ? -v.y : v.y;
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            const cf v = src.get(b + r * NB);
+            xr[r] = v.x;
+            xi[r] = v.y;
+        }
+    }
+    if constexpr (S > 0) {
+        const int k = b & (P - 1);
+        const float2* w = tws + OFF + k;
+#pragma unroll
+        for (int r = 1; r < 16; r++) {
+            const float2 wr = TWS_SMEM ? w[(r - 1) * P] : __ldg(&w[(r - 1) * P]);
+            fafct::cmul_inplace(xr[r], xi[r], wr.x, wr.y);
+        }
+    }
+    // the A tiles alias the workspace: every read of it ends first
+    if constexpr (Src::kSmem) __syncthreads();
+    // ---- per-row power-of-two scale into FP16 range, hi / lo split, A rows
+    float m = 0.f;
+#pragma unroll
+    for (int r = 0; r < 16; r++) m = fmaxf(m, fmaxf(fabsf(xr[r]), fabsf(xi[r])));
+    const int e = ((__float_as_int(m) >> 23) & 0xff) - 127;
+    const int sh = max(-64, min(64, 13 - e));
+    const float s = __int_as_float((127 + sh) << 23);
+    const float inv = __int_as_float((127 - sh) << 23);
+    {
+        const uint32_t row_off = (uint32_t)((c.row & 7) * 16 + (c.row >> 3) * kSbo);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {  // K chunks: re[0..7], re[8..15], im[0..7], im[8..15]
+            const float* v = q < 2 ? &xr[8 * q] : &xi[8 * (q - 2)];
+            uint32_t h[4], l[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) split2(v[2 * j] * s, v[2 * j + 1] * s, h[j], l[j]);
+            const uint32_t ah = c.a_hi + row_off + q * kALbo;
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ah), "r"(h[0]),
+                         "r"(h[1]), "r"(h[2]), "r"(h[3])
+                         : "memory");
+            asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(ah + kTileBytes),
+                         "r"(l[0]), "r"(l[1]), "r"(l[2]), "r"(l[3])
+                         : "memory");
+        }
+    }
+    fence_async_smem();
+    fence_before_sync();
+    asm volatile("bar.sync %0, 128;" ::"r"(1 + (int)(threadIdx.x >> 7)) : "memory");
+    // ---- one thread issues D = A_hi B_hi + A_hi B_lo + A_lo B_hi (K = 2 x 16)
+    if (c.leader) {
+        fence_after_sync();
+        const uint64_t ah = sdesc(c.a_hi, kALbo, kSbo);
+        const uint64_t al = sdesc(c.a_hi + kTileBytes, kALbo, kSbo);
+        const uint64_t bh = sdesc(c.b_hi, kBLbo, kSbo);
+        const uint64_t bl = sdesc(c.b_hi + 2048, kBLbo, kSbo);
+        constexpr uint64_t ka = (2 * kALbo) >> 4, kb = (2 * kBLbo) >> 4;  // second K step
+        mma(c.tmem, ah, bh, 0);
+        mma(c.tmem, ah + ka, bh + kb, 1);
+        mma(c.tmem, ah, bl, 1);
+        mma(c.tmem, ah + ka, bl + kb, 1);
+        mma(c.tmem, al, bh, 1);
+        mma(c.tmem, al + ka, bh + kb, 1);
+        commit(c.bar);
+    }
+    if (!wait_bounded(c.bar, c.phase)) atomicOr(c.err, 1);
+    c.phase ^= 1;
+    fence_after_sync();
+    {
+        uint32_t d[32];
+        tmem_ld32(c.tmem_ld, d);
+#pragma unroll
+        for (int r = 0; r < 16; r++) {
+            xr[r] = __uint_as_float(d[r]) * inv;
+            xi[r] = __uint_as_float(d[16 + r]) * inv;
+        }
+    }
+    // every warpgroup's tiles are consumed before outputs overwrite the workspace
+    fence_before_sync();
+    __syncthreads();
+    // ---- outputs in natural order (the MMA computes the plain DFT)
+    const int k = b & (P - 1);
+    const int base = ((b >> LP) << (LP + 4)) + k;
+    if constexpr (fafct::is_fast<Snk>::value && (P % 16 == 0 || P == 1)) {
+        float2* p = fafct::fast_ptr(snk) + fafct::pad2(base);
+        constexpr int step = (P % 16 == 0) ? P + P / 16 : 1;
+#pragma unroll
+        for (int r = 0; r < 16; r++) p[r * step] = make_float2(xr[r], xi[r]);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 16; r++) snk.put(base + r * P, cf{xr[r], xi[r]});
+    }
+    if constexpr (Snk::kSmem) __syncthreads();
+}
+
+template <int N, int S, bool TWS, class Src, class Snk>
+__device__ __forceinline__ void any_stage(float (&xr)[16], float (&xi)[16], int t,
+                                          const float2* __restrict__ tws, const Src& src,
+                                          const Snk& snk, Ctx& c) {
+    if constexpr (P2<N>::radix(S) == 16)
+        tc_stage<N, S, TWS>(xr, xi, t, tws, src, snk, c);
+    else
+        fafct::ct_stage<N, S, TWS>(xr, xi, t, tws, src, snk, CtaSync{});
+}
+
+template <int N, int S, bool TWS, class Src, class Snk>
+__device__ __forceinline__ void tc_run(float (&xr)[16], float (&xi)[16], int t, float2* ws,
+                                       const float2* __restrict__ tws, const Src& src,
+                                       const Snk& snk, Ctx& c) {
+    using Pl = P2<N>;
+    const SmemC mid{ws};
+    const LastC<Snk> last{snk};
+    if constexpr (Pl::NS == 1) {
+        any_stage<N, 0, TWS>(xr, xi, t, tws, src, last, c);
+    } else if constexpr (S == 0) {
+        any_stage<N, 0, TWS>(xr, xi, t, tws, src, mid, c);
+        tc_run<N, 1, TWS>(xr, xi, t, ws, tws, mid, snk, c);
+    } else if constexpr (S == Pl::NS - 1) {
+        any_stage<N, S, TWS>(xr, xi, t, tws, mid, last, c);
+    } else {
+        any_stage<N, S, TWS>(xr, xi, t, tws, mid, mid, c);
+        tc_run<N, S + 1, TWS>(xr, xi, t, ws, tws, mid, snk, c);
+    }
+}
+
+// Bytes of shared memory past the twiddle table and the group workspaces.
+constexpr size_t kTailBytes = kBBytes + 8 * kWarpgroups + 16;
+
+template <int N>
+constexpr size_t smem_bytes() {
+    constexpr int G = kThreads / P2<N>::T;
+    return (size_t)CtCfg<N>::TWN * sizeof(float2) +
+           (size_t)G * group_stride(N, N, false) * sizeof(float2) + kTailBytes;
+}
+
+template <int N>
+__global__ void __launch_bounds__(kThreads, 1)
+    k2_c2c_tc(const float2* __restrict__ tws, const C2CArgs a, const uint4* __restrict__ gB,
+              int* err) {
+    static_assert(P2<N>::N16 >= 1, "needs at least one radix-16 stage");
+    constexpr int G = kThreads / P2<N>::T;
+    static_assert((size_t)G * group_stride(N, N, false) * sizeof(float2) >=
+                      (size_t)kWarpgroups * 2 * kTileBytes,
+                  "A tiles must fit in the workspace they alias");
+    extern __shared__ float4 smem4[];
+    float2* sm2 = reinterpret_cast<float2*>(smem4);
+    CtGroup<N> q(sm2, N, tws);
+    uint8_t* wsb = reinterpret_cast<uint8_t*>(sm2 + CtCfg<N>::TWN);
+    uint8_t* bsm = wsb + (size_t)G * group_stride(N, N, false) * sizeof(float2);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(bsm + kBBytes);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kWarpgroups);
+    const int wg = threadIdx.x >> 7, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < (int)(kBBytes / 16); i += blockDim.x)
+        reinterpret_cast<uint4*>(bsm)[i] = gB[i];
+    if (threadIdx.x < kWarpgroups)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bars[threadIdx.x]))
+                     : "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tslot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    Ctx c;
+    const uint32_t tbase = *tslot;
+    c.tmem = tbase + 32 * wg;
+    c.tmem_ld = tbase + ((uint32_t)(32 * (warp & 3)) << 16) + 32 * wg;
+    c.a_hi = smem_u32(wsb) + (uint32_t)wg * 2 * kTileBytes;
+    c.b_hi = smem_u32(bsm);
+    c.bar = &bars[wg];
+    c.phase = 0;
+    c.row = threadIdx.x & 127;
+    c.err = err;
+    c.leader = (threadIdx.x & 127) == 0;
+    float xr[16], xi[16];
+    const int fpe = a.interleaved ? 2 : 1;
+    CT_FOR_GROUPS(G, a.batch) {
+        const long long b = grp_ * G + q.g;
+        const bool live = b < a.batch;
+        const long long bi = live ? b : 0;
+        const long long io = bi * a.in_dist * fpe, oo = bi * a.out_dist * fpe;
+        SplitSrc src{a.in_re + io, a.interleaved ? nullptr : a.in_im + io, a.window, a.sgn,
+                     a.interleaved, live};
+        SplitSink snk{a.out_re + oo, a.interleaved ? nullptr : a.out_im + oo, a.scale, a.sgn,
+                      a.interleaved, live};
+        __syncthreads();  // the workspace is free (previous group done)
+        tc_run<N, 0, kTw<N>>(xr, xi, q.t, q.ws, q.tw, src, snk, c);
+    }
+    // release the accumulators once every MMA has completed
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase),
+                     "r"(kTmemCols)
+                     : "memory");
+}
+
+template <int N>
+cudaError_t launch_n(const float2* tws, const C2CArgs& a, const void* gB, int* err,
+                     cudaStream_t st) {
+    constexpr size_t smem = smem_bytes<N>();
+    cudaError_t e = prep(k2_c2c_tc<N>, smem);
+    if (e != cudaSuccess) return e;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    constexpr int G = kThreads / P2<N>::T;
+    const long long groups = (a.batch + G - 1) / G;
+    const unsigned grid = (unsigned)std::max(1LL, std::min(groups, (long long)sms));
+    k2_c2c_tc<N><<<grid, kThreads, smem, st>>>(tws, a, (const uint4*)gB, err);
+    return cudaGetLastError();
+}
+
+}  // namespace tc
+
+bool tc_supported(int log2n) { return log2n >= 8 && log2n <= 14; }
+
+cudaError_t launch_c2c_tc(int log2n, const float2* tws, const C2CArgs& a, const void* gB,
+                          int* err, cudaStream_t st) {
+    if (a.batch <= 0) return cudaSuccess;
+    switch (log2n) {
+    case 8: return tc::launch_n<256>(tws, a, gB, err, st);
+    case 9: return tc::launch_n<512>(tws, a, gB, err, st);
+    case 10: return tc::launch_n<1024>(tws, a, gB, err, st);
+    case 11: return tc::launch_n<2048>(tws, a, gB, err, st);
+    case 12: return tc::launch_n<4096>(tws, a, gB, err, st);
+    case 13: return tc::launch_n<8192>(tws, a, gB, err, st);
+    case 14: return tc::launch_n<16384>(tws, a, gB, err, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace fafk

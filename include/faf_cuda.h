@@ -8,6 +8,7 @@
  *   - batched execute: many transforms of one plan in one launch
  *   - uneven batches: transforms of different lengths in one persistent,
  *     CUDA-graph-captured launch (faf_uneven_*)
+ *   - the tensor-core precision form of C2C (FAF_FLAG_TENSOR_CORE)
  *
  * Pointers are plain `void *` / `float *` so the header needs no CUDA
  * include; a `void *stream` is a cudaStream_t.
@@ -21,6 +22,13 @@
 extern "C" {
 #endif
 
+/* ---- flags (bits >= 16: no overlap with the reference's FAF_FLAG_*) ------- */
+
+/* faf_create_fft: run the radix-16 stages of a power-of-two C2C (256 ..
+ * 16384 points) as FP16 tensor-core MMAs with hi + lo split operands and FP32
+ * accumulation (FP32-level accuracy).  Other sizes ignore the flag. */
+#define FAF_FLAG_TENSOR_CORE (1u << 16)
+
 /* ---- library / device --------------------------------------------------- */
 
 /* 1 if a CUDA device is usable, 0 otherwise (message in faf_get_error()). */
@@ -28,6 +36,10 @@ int faf_cuda_available(void);
 /* Name of the plan kind behind t ("c2c", "rader", "bluestein", "r2c", "c2r",
  * "pipeline", "stft", "c2c-4step", ...), or NULL. */
 const char *faf_cuda_plan_kind(const faf_transform *t);
+/* Tensor-core plans: 0 if every MMA wait of this plan's launches so far
+ * completed, 1 if one ran out of its bound (the results are then invalid);
+ * -1 if t is not a tensor-core plan.  Synchronises the plan's stream. */
+int faf_cuda_tc_status(const faf_transform *t);
 /* Number of kernel launches the last execute on this thread made. */
 int faf_cuda_last_launches(void);
 
