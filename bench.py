@@ -10,7 +10,7 @@ once, each output sample written once: 8 bytes per sample) and its fraction
 of the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload pipeline|r2c|c2c1024|c2c16384|stft|uneven|serve]
+                    [--workload pipeline|r2c|c2c1024|c2c16384|c2c16384tc|stft|uneven|serve]
 
 --workload serve replays a Poisson request trace (20k requests/s: 40% rfft
 of log-uniform sizes 256..65536 rounded to the recommended size, 30% the
@@ -68,6 +68,9 @@ WORKLOADS = {
                 16 * 1024, 5 * 1024 * 10),
     "c2c16384": ("C2C n=16384 batch 2048 forward (split planes), seed 3", 16384, 2048,
                  16 * 16384, 5 * 16384 * 14),
+    "c2c16384tc": ("C2C n=16384 batch 2048 forward, tensor-core form (radix-16 stages as FP16 "
+                   "hi+lo tcgen05 MMAs, FP32 accumulation), seed 3, 1% of entries x1e3",
+                   16384, 2048, 16 * 16384, 5 * 16384 * 14),
     "stft": ("STFT Hann 1024 hop 256, 64 signals x 2^18 samples, seed 4", 1024, 64,
              None, None),
     "uneven": ("uneven batch: 4096 C2C, lengths uniform over {12,17,31,60,240,1000,3072,6000,"
@@ -101,7 +104,7 @@ def make_inputs(workload, batch):
         rng = np.random.default_rng(seed)
         re = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
         im = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
-        if workload == "c2c16384":
+        if workload.startswith("c2c16384"):
             for a in (re, im):
                 a[rng.random(a.shape) < 0.01] *= 1e3
         return [re, im]
@@ -224,6 +227,8 @@ def build_transform(F, workload, torch):
         return t
     if workload == "r2c":
         return F.Transform.rfft(n)
+    if workload == "c2c16384tc":
+        return F.Transform.fft(n, flags=F.FLAG_TENSOR_CORE)
     if workload.startswith("c2c"):
         return F.Transform.fft(n)
     if workload == "stft":
@@ -344,6 +349,32 @@ def run_ours(args, rank, world, local_rank):
                  "launches_per_step": len(set(uneven_lengths(batch))),
                  "speedup_of_persistent": round(pms / ms_per_step, 3)}
 
+    if workload == "c2c16384tc":
+        # accuracy of the tensor-core form on a sample, and the plain CUDA-core
+        # path on the same data
+        k = 4
+        want = np.fft.fft(host_in[0][:k].astype(np.float64) + 1j * host_in[1][:k], axis=-1)
+        got = outs[0][:k].cpu().numpy() + 1j * outs[1][:k].cpu().numpy()
+        acc = {"rel_l2_vs_fp64": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
+               "sample": f"first {k} transforms", "tc_status": t.tc_status()}
+        tp = F.Transform.fft(n)
+        tp.set_stream(stream)
+        for _ in range(3):
+            run_step(F, tp, workload, ins, outs)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            run_step(F, tp, workload, ins, outs)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        pms = ev0.elapsed_time(ev1) / args.steps
+        plain = {"value": round(nbytes / (pms * 1e-3) / 1e9, 1), "ms_per_step": round(pms, 4),
+                 "speedup_of_tensor_core_form": round(pms / ms_per_step, 3)}
+        # three radix-16 stages x (16384 / 16) / 128 tiles x six 128x32x16 MMAs
+        tflops = batch * 3 * (16384 // 16 // 128) * 6 * 2 * 128 * 32 * 16 / (ms_per_step * 1e-3) / 1e12
+        acc["tensor_tflops"] = round(tflops, 1)
+        tp.close()
+
     # end to end through the public API with pinned host buffers
     host_pinned = [torch.from_numpy(a).pin_memory().numpy() for a in host_in]
     host_out = alloc_outputs(workload, batch, host_pinned[0], torch)
@@ -372,7 +403,8 @@ def run_ours(args, rank, world, local_rank):
                 "traffic": ncu_traffic(workload),
                 "algorithmic_bytes_per_launch": nbytes,
                 "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
-                           "uneven": "k_uneven"}.get(workload, "k2_c2c")}
+                           "uneven": "k_uneven_large", "c2c16384tc": "k2_c2c_tc"}.get(
+                               workload, "k2_c2c")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -407,8 +439,11 @@ def run_ours(args, rank, world, local_rank):
             "gpu_launches": launches,
             "clocks": sampler.result(),
         }
-        if plain is not None:
+        if plain is not None and workload == "uneven":
             line["plain_one_launch_per_length"] = plain
+        elif plain is not None:
+            line["plain_cuda_core_path"] = plain
+            line["accuracy"] = acc
         print(json.dumps(line), flush=True)
     t.close()
     t_e2e.close()

@@ -190,6 +190,94 @@ int ensure_stage(DevicePlan* p, size_t bytes) {
 
 int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t st);
 
+// Host buffers, large batches: the batch runs in chunks through a ring of
+// three device slots, host-to-device copies on one copy stream, kernels on
+// the plan's stream (in order, so plan scratch is never shared), and
+// device-to-host copies on a second copy stream.  Chunk i's input copy, chunk
+// i-1's kernel and chunk i-2's output copy overlap, and the two PCIe
+// directions run at once.  Events order each slot's reuse.
+constexpr int kSlots = 3;
+constexpr size_t kChunkMinBytes = 8u << 20;  // per-direction bytes below which one shot wins
+
+int ensure_copy_streams(DevicePlan* p) {
+    cudaError_t e = cudaSuccess;
+    if (!p->cp_h2d) e = cudaStreamCreateWithFlags(&p->cp_h2d, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !p->cp_d2h)
+        e = cudaStreamCreateWithFlags(&p->cp_d2h, cudaStreamNonBlocking);
+    for (int i = 0; i < kSlots && e == cudaSuccess; i++) {
+        if (!p->ev_h2d[i]) e = cudaEventCreateWithFlags(&p->ev_h2d[i], cudaEventDisableTiming);
+        if (e == cudaSuccess && !p->ev_kern[i])
+            e = cudaEventCreateWithFlags(&p->ev_kern[i], cudaEventDisableTiming);
+        if (e == cudaSuccess && !p->ev_d2h[i])
+            e = cudaEventCreateWithFlags(&p->ev_d2h[i], cudaEventDisableTiming);
+    }
+    return e == cudaSuccess ? 0 : cuda_fail(e, "copy streams");
+}
+
+int run_host_chunked(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t st,
+                     long long chunk) {
+    if (ensure_copy_streams(p) != 0) return -1;
+    const int nin = r.in_b ? 2 : 1, nout = r.out_b ? 2 : 1;
+    const size_t fin = span_floats(chunk, r.in_dist, r.in_len, r.in_fpe);
+    const size_t fout = span_floats(chunk, r.out_dist, r.out_len, r.out_fpe);
+    // slot layout, each plane rounded to 64 floats (256 bytes)
+    auto up = [](size_t f) { return (f + 63) & ~(size_t)63; };
+    const size_t slot_floats = up(fin) * nin + up(fout) * nout;
+    if (ensure_stage(p, kSlots * slot_floats * sizeof(float)) != 0) return -1;
+    cudaError_t e = cudaSuccess;
+    // the copy streams start after work already queued on the plan's stream
+    e = cudaEventRecord(p->ev_kern[0], st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(p->cp_h2d, p->ev_kern[0], 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(p->cp_d2h, p->ev_kern[0], 0);
+    int launches = 0;
+    const long long nchunks = (r.batch + chunk - 1) / chunk;
+    for (long long i = 0; i < nchunks && e == cudaSuccess; i++) {
+        const int s = (int)(i % kSlots);
+        const long long b0 = i * chunk, cb = std::min(chunk, r.batch - b0);
+        float* slot = (float*)p->d_stage + (size_t)s * slot_floats;
+        Request d = r;
+        d.batch = cb;
+        d.in_a = slot;
+        d.in_b = r.in_b ? slot + up(fin) : nullptr;
+        d.out_a = slot + up(fin) * nin;
+        d.out_b = r.out_b ? d.out_a + up(fout) : nullptr;
+        const size_t ioff = (size_t)b0 * r.in_dist * r.in_fpe;
+        const size_t ooff = (size_t)b0 * r.out_dist * r.out_fpe;
+        const size_t cin = span_floats(cb, r.in_dist, r.in_len, r.in_fpe) * sizeof(float);
+        const size_t cout = span_floats(cb, r.out_dist, r.out_len, r.out_fpe) * sizeof(float);
+        // input copy: the slot's previous kernel has read its inputs
+        if (i >= kSlots) e = cudaStreamWaitEvent(p->cp_h2d, p->ev_kern[s], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync((void*)d.in_a, r.in_a + ioff, cin, cudaMemcpyHostToDevice,
+                                p->cp_h2d);
+        if (e == cudaSuccess && r.in_b)
+            e = cudaMemcpyAsync((void*)d.in_b, r.in_b + ioff, cin, cudaMemcpyHostToDevice,
+                                p->cp_h2d);
+        if (e == cudaSuccess) e = cudaEventRecord(p->ev_h2d[s], p->cp_h2d);
+        // kernel: inputs arrived, the slot's previous outputs have left
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, p->ev_h2d[s], 0);
+        if (e == cudaSuccess && i >= kSlots) e = cudaStreamWaitEvent(st, p->ev_d2h[s], 0);
+        if (e != cudaSuccess) break;
+        if (run_device(t, p, d, st) != 0) return -1;
+        launches += faf_cuda_last_launches();
+        e = cudaEventRecord(p->ev_kern[s], st);
+        // output copy
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(p->cp_d2h, p->ev_kern[s], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(r.out_a + ooff, d.out_a, cout, cudaMemcpyDeviceToHost,
+                                p->cp_d2h);
+        if (e == cudaSuccess && r.out_b)
+            e = cudaMemcpyAsync(r.out_b + ooff, d.out_b, cout, cudaMemcpyDeviceToHost,
+                                p->cp_d2h);
+        if (e == cudaSuccess) e = cudaEventRecord(p->ev_d2h[s], p->cp_d2h);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(p->cp_d2h);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "chunked host execute");
+    note_launches(launches);
+    return 0;
+}
+
 int execute_request(const faf_transform* t, Request& r) {
     DevicePlan* p = plan_of(t);
     if (!p) return fail("transform has no CUDA plan");
@@ -222,6 +310,16 @@ int execute_request(const faf_transform* t, Request& r) {
         const size_t fout = span_floats(r.batch, r.out_dist, r.out_len, r.out_fpe);
         const int nin = r.in_b ? 2 : 1, nout = r.out_b ? 2 : 1;
         const size_t total = (fin * nin + fout * nout) * sizeof(float) + 256;
+        const size_t per_dir = std::max(fin * nin, fout * nout) * sizeof(float);
+        if (per_dir >= 2 * kChunkMinBytes && r.batch >= 8) {
+            // about 16 chunks, none below kChunkMinBytes per direction
+            long long chunk = (r.batch + 15) / 16;
+            const size_t per_t = std::max(per_dir / (size_t)r.batch, (size_t)1);
+            chunk = std::max<long long>(chunk, (long long)(kChunkMinBytes / per_t));
+            chunk = std::min<long long>(chunk, r.batch);
+            rc = run_host_chunked(t, p, r, st, chunk);
+            goto done;
+        }
         if ((rc = ensure_stage(p, total)) != 0) goto done;
         {
             float* base = (float*)p->d_stage;

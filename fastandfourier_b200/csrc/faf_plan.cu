@@ -312,6 +312,13 @@ void plan_free(DevicePlan* p) {
     cudaFree(p->d_stage);
     cudaFree(p->d_scratch);
     cudaFree(p->d_work);
+    if (p->cp_h2d) cudaStreamDestroy(p->cp_h2d);
+    if (p->cp_d2h) cudaStreamDestroy(p->cp_d2h);
+    for (int i = 0; i < 3; i++) {
+        if (p->ev_h2d[i]) cudaEventDestroy(p->ev_h2d[i]);
+        if (p->ev_kern[i]) cudaEventDestroy(p->ev_kern[i]);
+        if (p->ev_d2h[i]) cudaEventDestroy(p->ev_d2h[i]);
+    }
     delete p;
 }
 

@@ -89,6 +89,9 @@ struct DevicePlan {
     std::mutex mu;
     void* d_stage = nullptr;
     size_t stage_bytes = 0;
+    // chunked host-buffer path: copy streams and per-slot events (lazy)
+    cudaStream_t cp_h2d = nullptr, cp_d2h = nullptr;
+    cudaEvent_t ev_h2d[3] = {}, ev_kern[3] = {}, ev_d2h[3] = {};
     void* d_scratch = nullptr;
     size_t scratch_bytes = 0;
 };
