@@ -288,6 +288,17 @@ def alloc_outputs(workload, batch, like, torch):
         return [mk((total,)), mk((total,))]
 
 
+def max_over_ranks(x, dist, device):
+    """Max of a per-rank float over all ranks (identity without a process
+    group); every rank calls it at the same point."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import fastandfourier_b200 as F
@@ -328,9 +339,7 @@ def run_ours(args, rank, world, local_rank):
     ms = ev0.elapsed_time(ev1)
     if dist:
         dist.barrier()
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, dist, "cuda")
     ms_per_step = ms / args.steps
     value = world * nbytes / (ms_per_step * 1e-3) / 1e9
     plain = None
@@ -387,11 +396,7 @@ def run_ours(args, rank, world, local_rank):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         run_step(F, t_e2e, workload, host_pinned, host_out)
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, dist, "cuda")
     h2d = sum(a.nbytes for a in host_pinned)
     d2h = sum(a.nbytes for a in host_out)
     e2e_value = world * nbytes / e2e_s / 1e9

@@ -1,0 +1,68 @@
+"""The multi-rank plumbing of bench.py on the CPU: world_size-2 `gloo` ranks
+take the max over ranks of their timings, and under torchrun the reference
+arm runs on rank 0 alone (the other rank exits 0 without output)."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out_dir):
+    import datetime
+
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    mine = 10.0 + 5.0 * rank  # rank 1 is the slow one
+    got = bench.max_over_ranks(mine, dist, "cpu")
+    dist.barrier()
+    with open(os.path.join(out_dir, f"r{rank}.txt"), "w") as f:
+        f.write(repr(got))
+    dist.destroy_process_group()
+
+
+def test_max_over_ranks_gloo(tmp_path):
+    import torch.multiprocessing as mp
+    port = _free_port()
+    mp.start_processes(_rank_main, args=(2, port, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    vals = [float(open(os.path.join(tmp_path, f"r{r}.txt")).read()) for r in range(2)]
+    assert vals == [15.0, 15.0]
+
+
+def test_max_over_ranks_single_process():
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
+
+
+def test_reference_arm_rank0_only():
+    sys.path.insert(0, ROOT)
+    from oracle import refimpl
+    if not refimpl.available() and not os.path.isdir(refimpl.REFERENCE_SRC):
+        pytest.skip("reference library not built")
+    port = _free_port()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+           "--master-addr", "127.0.0.1", "--master-port", str(port),
+           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--workload", "c2c1024",
+           "--gpus", "2", "--steps", "1", "--warmup", "1"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
