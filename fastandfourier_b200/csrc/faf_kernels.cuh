@@ -119,6 +119,29 @@ cudaError_t launch_pot2(int kind, int log2n, const float2* tws, const void* args
 // Shared-memory bytes the twiddle table of a log2n kernel adds to each CTA.
 size_t pot2_table_smem(int log2n);
 
+// Batched multi-CTA four-step for power-of-two lengths above one CTA
+// (k_large_pot2.cu): columns, then rows, through a chunked scratch.
+struct Large2Args {
+    const float* in_re;
+    const float* in_im;
+    float* out_re;
+    float* out_im;
+    long long in_dist, out_dist;  // element distance between transforms ...
+    const long long* offs;        // ... or per-transform element offsets (in and out)
+    long long batch;
+    float scale, sgn;
+    const float2* tws1;           // per-stage tables of the N1- and N2-point engines
+    const float2* tws2;
+    const float2* twm;            // middle twiddles [k1 * N2 + col]
+    float* scratch;               // scratch_transforms x 2 n floats
+    long long scratch_transforms;
+};
+bool large_pot2_supported(int n1, int n2);
+long long large_pot2_chunk(long long n);       // transforms per scratch chunk
+int large_pot2_launches(int n1, int n2, long long batch);
+cudaError_t large_pot2_prepare(int n1, int n2);  // kernel attributes, before any capture
+cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st);
+
 // Tensor-core precision form of the power-of-two C2C (k_tc.cu).
 bool tc_supported(int log2n);
 cudaError_t launch_c2c_tc(int log2n, const float2* tws, const C2CArgs& a, const void* gB,

@@ -637,12 +637,50 @@ static cudaError_t run_large(DevicePlan* p, int kind, const void* args, long lon
     return fafk::launch_large(kind, a, args, batch, grid, st);
 }
 
+// Power-of-two lengths above one CTA: the multi-CTA two-pass four-step
+// through a chunked scratch (p->d_work).
+static cudaError_t run_large_pot2(DevicePlan* p, const float* in_re, const float* in_im,
+                                  float* out_re, float* out_im, long long batch,
+                                  long long in_dist, long long out_dist, float sgn,
+                                  cudaStream_t st) {
+    const long long n = (long long)p->n1 * p->n2;
+    const long long chunk = std::min(batch, fafk::large_pot2_chunk(n));
+    const size_t bytes = (size_t)chunk * 2 * (size_t)n * sizeof(float);
+    {
+        std::lock_guard<std::mutex> lk(p->mu);
+        if (p->work_bytes < bytes) {
+            cudaFree(p->d_work);
+            p->d_work = nullptr;
+            p->work_bytes = 0;
+            cudaError_t e = cudaMalloc(&p->d_work, bytes);
+            if (e != cudaSuccess) return e;
+            p->work_bytes = bytes;
+        }
+    }
+    fafk::Large2Args a;
+    std::memset(&a, 0, sizeof a);
+    a.in_re = in_re; a.in_im = in_im; a.out_re = out_re; a.out_im = out_im;
+    a.in_dist = in_dist; a.out_dist = out_dist; a.offs = nullptr; a.batch = batch;
+    a.scale = p->scale; a.sgn = sgn;
+    a.tws1 = p->f1.d_tws; a.tws2 = p->f2.d_tws; a.twm = p->d_tw_big;
+    a.scratch = (float*)p->d_work;
+    a.scratch_transforms = chunk;
+    return fafk::launch_large_pot2(p->n1, p->n2, a, st);
+}
+
+bool large_pot2_plan(const DevicePlan* p) {
+    return p->large && p->f1.ct_log2 && p->f2.ct_log2 && fafk::large_pot2_supported(p->n1, p->n2);
+}
+
 cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, float* out_re,
                      float* out_im, long long batch, long long in_dist, long long out_dist,
                      bool interleaved, const float* window, cudaStream_t st) {
     const float sgn = p->inverse ? -1.0f : 1.0f;
     if (p->kind == Kind::C2C_LARGE) {
         if (interleaved || window) return cudaErrorNotSupported;
+        if (large_pot2_plan(p))
+            return run_large_pot2(p, in_re, in_im, out_re, out_im, batch, in_dist, out_dist, sgn,
+                                  st);
         fafk::C2CArgs a;
         std::memset(&a, 0, sizeof a);
         a.in_re = in_re; a.in_im = in_im; a.out_re = out_re; a.out_im = out_im;

@@ -122,6 +122,8 @@ bool build_large(DevicePlan* p, int n, std::string& err);
 // a power of two (so that groups tile a power-of-two CTA exactly).
 int padded_threads(int m);
 bool needs_four_step(int n);
+// Power-of-two four-step plan that the multi-CTA two-pass kernels serve.
+bool large_pot2_plan(const DevicePlan* p);
 
 // Host FFT in double precision (table generation only).
 void host_dft_fp64(std::vector<double>& re, std::vector<double>& im);

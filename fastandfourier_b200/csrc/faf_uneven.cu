@@ -189,13 +189,18 @@ cudaError_t occupancy(K k, int threads, size_t smem, int* per_sm) {
 
 using fafp::DevicePlan;
 
-// One launch of k_uneven_large: the transforms of one long length.
+// The transforms of one long length: either the multi-CTA two-pass
+// four-step (power-of-two lengths, over a per-class offset list), or one
+// launch of k_uneven_large (one transform per CTA).
 struct LargeLaunch {
     fafk::LargeArgs la;
     int first;   // into items
     int count;
     float scale;
     int grid;
+    bool pot2 = false;
+    DevicePlan* plan = nullptr;
+    long long* d_offs = nullptr;  // pot2: element offset of each transform of the class
 };
 
 struct faf_uneven {
@@ -285,6 +290,7 @@ int build_schedule(faf_uneven* u) {
     u->classes.clear();
     u->tasks.clear();
     u->items.clear();
+    for (auto& L : u->large) cudaFree(L.d_offs);
     u->large.clear();
     std::map<int, std::vector<int>> by_len;
     for (size_t i = 0; i < u->count; i++) by_len[(int)u->lengths[i]].push_back((int)i);
@@ -299,12 +305,16 @@ int build_schedule(faf_uneven* u) {
         const float scale = norm_scale(u->norm, u->inverse, (size_t)n);
         if (u->large_plans.count(n)) {
             LargeLaunch L;
-            L.la = large_args(u->large_plans[n]);
+            L.plan = u->large_plans[n];
+            L.la = large_args(L.plan);
             L.first = 0;  // set below, after the small-class items
             L.count = (int)ids.size();
             L.scale = scale;
             L.grid = std::min(sms, L.count);
-            scratch = std::max(scratch, (size_t)L.grid * 2 * (size_t)n);
+            L.pot2 = fafp::large_pot2_plan(L.plan);
+            const long long per = L.pot2 ? std::min<long long>(L.count, fafk::large_pot2_chunk(n))
+                                         : (long long)L.grid;
+            scratch = std::max(scratch, (size_t)per * 2 * (size_t)n);
             u->large.push_back(L);
             continue;
         }
@@ -351,6 +361,12 @@ int build_schedule(faf_uneven* u) {
         L.first = (int)u->items.size();
         const std::vector<int>& ids = by_len[L.la.n1 * L.la.n2];
         u->items.insert(u->items.end(), ids.begin(), ids.end());
+        if (L.pot2) {
+            std::vector<long long> offs;
+            for (int id : ids) offs.push_back(u->offsets_h[id]);
+            cudaError_t e2 = upload_vec(&L.d_offs, offs);
+            if (e2 != cudaSuccess) return cuda_fail(e2, "uneven four-step offsets");
+        }
     }
     u->smem_gen = std::max<size_t>(smem_gen, 16);
     u->smem_rad = std::max<size_t>(smem_rad, 16);
@@ -362,9 +378,9 @@ int build_schedule(faf_uneven* u) {
                              &per_rad)) != cudaSuccess)
         return cuda_fail(e, "uneven kernel attributes");
     for (auto& L : u->large) {
-        if ((e = prep(fafk::k_uneven_large, fafk::large_smem(L.la, fafk::kLargeThreads))) !=
-            cudaSuccess)
-            return cuda_fail(e, "uneven four-step kernel attributes");
+        e = L.pot2 ? fafk::large_pot2_prepare(L.la.n1, L.la.n2)
+                   : prep(fafk::k_uneven_large, fafk::large_smem(L.la, fafk::kLargeThreads));
+        if (e != cudaSuccess) return cuda_fail(e, "uneven four-step kernel attributes");
     }
     u->grid_gen = std::min(sms * per_gen, u->ntasks_gen);
     u->grid_rad = std::min(sms * std::min(per_rad, u->rad_per_sm), u->ntasks_rad);
@@ -420,6 +436,20 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
             return e;
     }
     for (const LargeLaunch& L : u->large) {
+        if (L.pot2) {
+            fafk::Large2Args a2;
+            memset(&a2, 0, sizeof a2);
+            a2.in_re = b.in_re; a2.in_im = b.in_im; a2.out_re = b.out_re; a2.out_im = b.out_im;
+            a2.offs = L.d_offs;
+            a2.batch = L.count;
+            a2.scale = L.scale;
+            a2.sgn = u->inverse ? -1.0f : 1.0f;
+            a2.tws1 = L.plan->f1.d_tws; a2.tws2 = L.plan->f2.d_tws; a2.twm = L.plan->d_tw_big;
+            a2.scratch = u->d_scratch;
+            a2.scratch_transforms = fafk::large_pot2_chunk((long long)L.la.n1 * L.la.n2);
+            if ((e = fafk::launch_large_pot2(L.la.n1, L.la.n2, a2, st)) != cudaSuccess) return e;
+            continue;
+        }
         fafk::LargeArgs la = L.la;
         la.scratch = u->d_scratch;
         la.cta_floats = 2LL * la.n1 * la.n2;
@@ -448,7 +478,10 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
 }
 
 int launches_per_run(const faf_uneven* u) {
-    return (int)u->large.size() + (u->grid_gen > 0) + (u->grid_rad > 0);
+    int k = (u->grid_gen > 0) + (u->grid_rad > 0);
+    for (const LargeLaunch& L : u->large)
+        k += L.pot2 ? fafk::large_pot2_launches(L.la.n1, L.la.n2, L.count) : 1;
+    return k;
 }
 
 cudaError_t capture(faf_uneven* u, const Bufs& b) {
@@ -670,6 +703,7 @@ extern "C" void faf_uneven_destroy(faf_uneven* u) {
     for (auto& kv : u->large_plans)
         if (!u->plans.count(kv.first) || u->plans[kv.first] != kv.second) fafp::plan_free(kv.second);
     for (auto& kv : u->plans) fafp::plan_free(kv.second);
+    for (auto& L : u->large) cudaFree(L.d_offs);
     cudaFree(u->d_classes);
     cudaFree(u->d_tasks);
     cudaFree(u->d_items);
