@@ -41,6 +41,7 @@ struct C2CArgs {
     float sgn;            // +1 forward, -1 inverse (conjugation trick)
     int interleaved;
     const float* window;  // optional per-sample real window (STFT frame), or NULL
+    const long long* offs = nullptr;  // per-transform element offsets (in and out), or NULL
 };
 
 struct RealArgs {  // R2C / C2R / pipeline / STFT
@@ -118,6 +119,9 @@ cudaError_t launch_pot2(int kind, int log2n, const float2* tws, const void* args
                         const Geometry& g, cudaStream_t st);
 // Shared-memory bytes the twiddle table of a log2n kernel adds to each CTA.
 size_t pot2_table_smem(int log2n);
+// Kernel attributes of the compile-time C2C kernel for geometry g (before any
+// stream capture reaches its launch).
+cudaError_t prepare_pot2_c2c(int log2n, const Geometry& g);
 
 // Batched multi-CTA four-step for power-of-two lengths above one CTA
 // (k_large_pot2.cu): columns, then rows, through a chunked scratch.

@@ -203,6 +203,17 @@ struct LargeLaunch {
     long long* d_offs = nullptr;  // pot2: element offset of each transform of the class
 };
 
+// A power-of-two class (256..16384 points): the compile-time engine over
+// the class's offset list, one batched launch.
+struct Pot2Launch {
+    int log2n;
+    const float2* tws;
+    float scale;
+    int count;
+    fafk::Geometry g;
+    long long* d_offs = nullptr;
+};
+
 struct faf_uneven {
     int device = 0;
     size_t count = 0;
@@ -220,6 +231,7 @@ struct faf_uneven {
     int ntasks_gen = 0, ntasks_rad = 0;
     std::vector<int> items;
     std::vector<LargeLaunch> large;
+    std::vector<Pot2Launch> pot2;
     fafk::UnevenClass* d_classes = nullptr;
     fafk::UnevenTask* d_tasks = nullptr;
     int* d_items = nullptr;
@@ -292,6 +304,8 @@ int build_schedule(faf_uneven* u) {
     u->items.clear();
     for (auto& L : u->large) cudaFree(L.d_offs);
     u->large.clear();
+    for (auto& P : u->pot2) cudaFree(P.d_offs);
+    u->pot2.clear();
     std::map<int, std::vector<int>> by_len;
     for (size_t i = 0; i < u->count; i++) by_len[(int)u->lengths[i]].push_back((int)i);
     const int sms = sm_count();
@@ -316,6 +330,24 @@ int build_schedule(faf_uneven* u) {
                                          : (long long)L.grid;
             scratch = std::max(scratch, (size_t)per * 2 * (size_t)n);
             u->large.push_back(L);
+            continue;
+        }
+        if (p->kind == fafp::Kind::C2C && p->inner.ct_log2 >= 8 && !p->tc) {
+            Pot2Launch P;
+            P.log2n = p->inner.ct_log2;
+            P.tws = p->inner.d_tws;
+            P.scale = scale;
+            P.count = (int)ids.size();
+            P.g = fafp::geometry_ct(p->inner, n, P.count);
+            std::vector<long long> offs;
+            for (int id : ids) offs.push_back(u->offsets_h[id]);
+            cudaError_t e2 = upload_vec(&P.d_offs, offs);
+            if (e2 == cudaSuccess) e2 = fafk::prepare_pot2_c2c(P.log2n, P.g);
+            if (e2 != cudaSuccess) {
+                cudaFree(P.d_offs);
+                return cuda_fail(e2, "uneven power-of-two class");
+            }
+            u->pot2.push_back(P);
             continue;
         }
         fafk::UnevenClass c;
@@ -428,7 +460,7 @@ fafk::UnevenArgs small_args(faf_uneven* u, const Bufs& b, bool rader) {
 cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(u->d_counter, 0, 2 * sizeof(int), st);
     if (e != cudaSuccess) return e;
-    const bool fork = !u->large.empty() && (u->grid_gen > 0 || u->grid_rad > 0);
+    const bool fork = !u->large.empty() && (u->grid_gen > 0 || u->grid_rad > 0 || !u->pot2.empty());
     cudaStream_t ss = fork ? u->side_stream : st;
     if (fork) {
         if ((e = cudaEventRecord(u->ev_fork, st)) != cudaSuccess ||
@@ -459,6 +491,17 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
                                fafk::large_smem(la, fafk::kLargeThreads), st>>>(la, a);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
+    for (const Pot2Launch& P : u->pot2) {
+        fafk::C2CArgs a;
+        memset(&a, 0, sizeof a);
+        a.in_re = b.in_re; a.in_im = b.in_im; a.out_re = b.out_re; a.out_im = b.out_im;
+        a.in_dist = a.out_dist = 1LL << P.log2n;
+        a.batch = P.count;
+        a.scale = P.scale;
+        a.sgn = u->inverse ? -1.0f : 1.0f;
+        a.offs = P.d_offs;
+        if ((e = fafk::launch_pot2(0, P.log2n, P.tws, &a, P.g, ss)) != cudaSuccess) return e;
+    }
     if (u->grid_gen > 0) {
         fafk::k_uneven_generic<<<u->grid_gen, fafk::kUnevenThreads, u->smem_gen, ss>>>(
             small_args(u, b, false));
@@ -478,7 +521,7 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
 }
 
 int launches_per_run(const faf_uneven* u) {
-    int k = (u->grid_gen > 0) + (u->grid_rad > 0);
+    int k = (u->grid_gen > 0) + (u->grid_rad > 0) + (int)u->pot2.size();
     for (const LargeLaunch& L : u->large)
         k += L.pot2 ? fafk::large_pot2_launches(L.la.n1, L.la.n2, L.count) : 1;
     return k;
@@ -704,6 +747,7 @@ extern "C" void faf_uneven_destroy(faf_uneven* u) {
         if (!u->plans.count(kv.first) || u->plans[kv.first] != kv.second) fafp::plan_free(kv.second);
     for (auto& kv : u->plans) fafp::plan_free(kv.second);
     for (auto& L : u->large) cudaFree(L.d_offs);
+    for (auto& P : u->pot2) cudaFree(P.d_offs);
     cudaFree(u->d_classes);
     cudaFree(u->d_tasks);
     cudaFree(u->d_items);

@@ -52,7 +52,8 @@ __global__ void __launch_bounds__(1024) k2_c2c(const float2* __restrict__ tws, c
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        const long long io = bi * a.in_dist * fpe, oo = bi * a.out_dist * fpe;
+        const long long io = (a.offs ? a.offs[bi] : bi * a.in_dist) * fpe;
+        const long long oo = (a.offs ? a.offs[bi] : bi * a.out_dist) * fpe;
         SplitSrc src{a.in_re + io, a.interleaved ? nullptr : a.in_im + io, a.window, a.sgn,
                      a.interleaved, live};
         SplitSink snk{a.out_re + oo, a.interleaved ? nullptr : a.out_im + oo, a.scale, a.sgn,
@@ -344,6 +345,28 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
         return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+template <int N>
+static cudaError_t prepare_c2c_n(const Geometry& g) {
+    return prep(k2_c2c<N>, g.smem + tw_bytes<N>());
+}
+
+cudaError_t prepare_pot2_c2c(int log2n, const Geometry& g) {
+    switch (log2n) {
+    case 4: return prepare_c2c_n<16>(g);
+    case 5: return prepare_c2c_n<32>(g);
+    case 6: return prepare_c2c_n<64>(g);
+    case 7: return prepare_c2c_n<128>(g);
+    case 8: return prepare_c2c_n<256>(g);
+    case 9: return prepare_c2c_n<512>(g);
+    case 10: return prepare_c2c_n<1024>(g);
+    case 11: return prepare_c2c_n<2048>(g);
+    case 12: return prepare_c2c_n<4096>(g);
+    case 13: return prepare_c2c_n<8192>(g);
+    case 14: return prepare_c2c_n<16384>(g);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 size_t pot2_table_smem(int log2n) {
