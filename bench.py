@@ -357,6 +357,33 @@ def run_ours(args, rank, world, local_rank):
         plain = {"value": round(nbytes / (pms * 1e-3) / 1e9, 1), "ms_per_step": round(pms, 4),
                  "launches_per_step": len(set(uneven_lengths(batch))),
                  "speedup_of_persistent": round(pms / ms_per_step, 3)}
+        # the tensor-core form of the same graph, with its error vs FP64
+        ttc = F.Uneven(uneven_lengths(batch), measure=True, tensor_core=True)
+        ttc.set_stream(stream)
+        for _ in range(3):
+            run_step(F, ttc, workload, ins, outs)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            run_step(F, ttc, workload, ins, outs)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        tms = ev0.elapsed_time(ev1) / args.steps
+        ls = uneven_lengths(batch)
+        offs = np.concatenate([[0], np.cumsum(ls)])
+        errs = []
+        yr, yi = outs[0].cpu().numpy(), outs[1].cpu().numpy()
+        for j in range(0, len(ls), max(1, len(ls) // 16)):  # every size class
+            a, b = offs[j], offs[j + 1]
+            want = np.fft.fft(host_in[0][a:b].astype(np.float64) + 1j * host_in[1][a:b])
+            got = yr[a:b] + 1j * yi[a:b]
+            errs.append(float(np.linalg.norm(got - want) / np.linalg.norm(want)))
+        plain["tensor_core_form"] = {"value": round(nbytes / (tms * 1e-3) / 1e9, 1),
+                                     "ms_per_step": round(tms, 4),
+                                     "speedup_over_plain": round(pms / tms, 3),
+                                     "max_rel_l2_vs_fp64": max(errs),
+                                     "sample": f"{len(errs)} transforms across the lengths"}
+        ttc.close()
 
     if workload == "c2c16384tc":
         # accuracy of the tensor-core form on a sample, and the plain CUDA-core

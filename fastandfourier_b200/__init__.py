@@ -187,11 +187,12 @@ class Uneven:
     launch.  Ragged packed split planes (transform i at offset sum of the
     previous lengths)."""
 
-    def __init__(self, lengths, *, inverse=False, norm=N_DEFAULT, measure=False):
+    def __init__(self, lengths, *, inverse=False, norm=N_DEFAULT, measure=False,
+                 tensor_core=False):
         self.lengths = [int(n) for n in lengths]
         arr = (ctypes.c_size_t * len(self.lengths))(*self.lengths)
-        c = config(0, dir=DIR_INVERSE if inverse else DIR_FORWARD, norm=norm,
-                   flags=FLAG_MEASURE if measure else 0)
+        flags = (FLAG_MEASURE if measure else 0) | (FLAG_TENSOR_CORE if tensor_core else 0)
+        c = config(0, dir=DIR_INVERSE if inverse else DIR_FORWARD, norm=norm, flags=flags)
         self._p = C.lib().faf_uneven_create(arr, len(self.lengths), ctypes.byref(c))
         if not self._p:
             raise FafError(C.error())

@@ -148,6 +148,7 @@ cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t 
 
 // Tensor-core precision form of the power-of-two C2C (k_tc.cu).
 bool tc_supported(int log2n);
+cudaError_t prepare_c2c_tc(int log2n);  // kernel attributes, before any capture
 cudaError_t launch_c2c_tc(int log2n, const float2* tws, const C2CArgs& a, const void* gB,
                           int* err, cudaStream_t st);
 

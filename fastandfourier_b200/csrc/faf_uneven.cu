@@ -207,6 +207,7 @@ struct LargeLaunch {
 // the class's offset list, one batched launch.
 struct Pot2Launch {
     int log2n;
+    const DevicePlan* plan;  // tensor-core plans carry their B table and error flag
     const float2* tws;
     float scale;
     int count;
@@ -332,9 +333,10 @@ int build_schedule(faf_uneven* u) {
             u->large.push_back(L);
             continue;
         }
-        if (p->kind == fafp::Kind::C2C && p->inner.ct_log2 >= 8 && !p->tc) {
+        if (p->kind == fafp::Kind::C2C && p->inner.ct_log2 >= 8) {
             Pot2Launch P;
             P.log2n = p->inner.ct_log2;
+            P.plan = p;
             P.tws = p->inner.d_tws;
             P.scale = scale;
             P.count = (int)ids.size();
@@ -342,7 +344,8 @@ int build_schedule(faf_uneven* u) {
             std::vector<long long> offs;
             for (int id : ids) offs.push_back(u->offsets_h[id]);
             cudaError_t e2 = upload_vec(&P.d_offs, offs);
-            if (e2 == cudaSuccess) e2 = fafk::prepare_pot2_c2c(P.log2n, P.g);
+            if (e2 == cudaSuccess)
+                e2 = p->tc ? fafk::prepare_c2c_tc(P.log2n) : fafk::prepare_pot2_c2c(P.log2n, P.g);
             if (e2 != cudaSuccess) {
                 cudaFree(P.d_offs);
                 return cuda_fail(e2, "uneven power-of-two class");
@@ -500,7 +503,10 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
         a.scale = P.scale;
         a.sgn = u->inverse ? -1.0f : 1.0f;
         a.offs = P.d_offs;
-        if ((e = fafk::launch_pot2(0, P.log2n, P.tws, &a, P.g, ss)) != cudaSuccess) return e;
+        e = P.plan->tc ? fafk::launch_c2c_tc(P.log2n, P.tws, a, P.plan->d_tcB,
+                                             P.plan->d_tc_err, ss)
+                       : fafk::launch_pot2(0, P.log2n, P.tws, &a, P.g, ss);
+        if (e != cudaSuccess) return e;
     }
     if (u->grid_gen > 0) {
         fafk::k_uneven_generic<<<u->grid_gen, fafk::kUnevenThreads, u->smem_gen, ss>>>(
@@ -630,7 +636,8 @@ extern "C" faf_uneven* faf_uneven_create(const size_t* lengths, size_t count,
     for (size_t i = 0; i < count; i++) {
         const int n = (int)lengths[i];
         if (u->plans.count(n)) continue;
-        DevicePlan* p = fafp::plan_c2c(n, u->inverse, norm_scale(c.norm, u->inverse, n), 0, err);
+        DevicePlan* p = fafp::plan_c2c(n, u->inverse, norm_scale(c.norm, u->inverse, n),
+                                       c.flags & FAF_FLAG_TENSOR_CORE, err);
         if (!p) {
             fail("faf_uneven_create: plan for length %d: %s", n, err.c_str());
             faf_uneven_destroy(u);

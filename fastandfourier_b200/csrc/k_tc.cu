@@ -353,7 +353,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        const long long io = bi * a.in_dist * fpe, oo = bi * a.out_dist * fpe;
+        const long long io = (a.offs ? a.offs[bi] : bi * a.in_dist) * fpe;
+        const long long oo = (a.offs ? a.offs[bi] : bi * a.out_dist) * fpe;
         SplitSrc src{a.in_re + io, a.interleaved ? nullptr : a.in_im + io, a.window, a.sgn,
                      a.interleaved, live};
         SplitSink snk{a.out_re + oo, a.interleaved ? nullptr : a.out_im + oo, a.scale, a.sgn,
@@ -372,10 +373,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 template <int N>
+cudaError_t prepare_n() {
+    return prep(k2_c2c_tc<N>, smem_bytes<N>());
+}
+
+template <int N>
 cudaError_t launch_n(const float2* tws, const C2CArgs& a, const void* gB, int* err,
                      cudaStream_t st) {
     constexpr size_t smem = smem_bytes<N>();
-    cudaError_t e = prep(k2_c2c_tc<N>, smem);
+    cudaError_t e = prepare_n<N>();
     if (e != cudaSuccess) return e;
     static int sms = 0;
     if (!sms) {
@@ -394,6 +400,19 @@ cudaError_t launch_n(const float2* tws, const C2CArgs& a, const void* gB, int* e
 }  // namespace tc
 
 bool tc_supported(int log2n) { return log2n >= 8 && log2n <= 14; }
+
+cudaError_t prepare_c2c_tc(int log2n) {
+    switch (log2n) {
+    case 8: return tc::prepare_n<256>();
+    case 9: return tc::prepare_n<512>();
+    case 10: return tc::prepare_n<1024>();
+    case 11: return tc::prepare_n<2048>();
+    case 12: return tc::prepare_n<4096>();
+    case 13: return tc::prepare_n<8192>();
+    case 14: return tc::prepare_n<16384>();
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_c2c_tc(int log2n, const float2* tws, const C2CArgs& a, const void* gB,
                           int* err, cudaStream_t st) {

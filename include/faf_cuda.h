@@ -70,7 +70,8 @@ typedef struct faf_uneven faf_uneven;
 
 /* Plan `count` C2C transforms of the given lengths, each a legal
  * faf_create_fft size <= 65536 (5-smooth, codelet or Rader prime).  cfg gives
- * dir / norm / flags (n is ignored); FAF_FLAG_MEASURE runs the launch-shape
+ * dir / norm / flags (n is ignored); FAF_FLAG_TENSOR_CORE puts the power-of-two
+ * lengths 256..16384 on the tensor-core precision form; FAF_FLAG_MEASURE runs the launch-shape
  * autotuner on the plan's own workload.  Layout: split planes, ragged and
  * packed -- transform i starts at element offset sum_{j<i} lengths[j]. */
 faf_uneven *faf_uneven_create(const size_t *lengths, size_t count, const faf_config *cfg);

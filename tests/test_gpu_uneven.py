@@ -84,3 +84,20 @@ def test_uneven_new_buffers_recapture(cuda):
         yr, yi = torch.empty_like(dr), torch.empty_like(di)
         u.execute(dr, di, yr, yi)
         assert check_against_fp64(lengths, re, im, yr.cpu().numpy(), yi.cpu().numpy()) <= REL_L2_TOL
+
+
+def test_uneven_tensor_core_form(cuda):
+    """FAF_FLAG_TENSOR_CORE: the power-of-two classes run as FP16 hi+lo MMAs;
+    every transform stays within rel L2 1e-5 of FP64."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    rng = seeded(21)
+    lengths = list(rng.choice(CONFIG3_LENGTHS + [256, 1024, 4096], 120))
+    re, im = ragged(lengths, 22)
+    for r in (re, im):
+        r[rng.random(r.shape) < 0.01] *= 1e3
+    u = F.Uneven(lengths, tensor_core=True)
+    dr, di = torch.from_numpy(re).cuda(), torch.from_numpy(im).cuda()
+    yr, yi = torch.empty_like(dr), torch.empty_like(di)
+    u.execute(dr, di, yr, yi)
+    assert check_against_fp64(lengths, re, im, yr.cpu().numpy(), yi.cpu().numpy()) <= REL_L2_TOL
