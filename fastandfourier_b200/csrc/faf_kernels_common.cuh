@@ -71,13 +71,15 @@ struct SplitSink {
 };
 
 // z[k] = x[2k] + i x[2k+1] (R2C packing, reference src/faf_rfft.c:356-359).
+// Packed real pairs z[i] = x[2i] + i x[2i+1].  Every caller points a dead
+// transform (past the batch) at transform 0, so the loads need no guard;
+// its results are dropped by the sink.
 struct RealPairSrc {
     const float* x;
-    bool live;
+    bool live;  // unused by the loads (kept for the callers' symmetry)
     bool vec;
     static constexpr bool kSmem = false;
     __device__ __forceinline__ cf get(int i) const {
-        if (!live) return cf{0.f, 0.f};
         if (vec) {
             float2 v = __ldcs(reinterpret_cast<const float2*>(x) + i);
             return cf{v.x, v.y};
@@ -287,28 +289,42 @@ struct ScatterSink {
 // Spectral ops of the fused pipeline on bin k (reference src/chirp.c:421-471,
 // src/faf_core.c:150-166): CONJ negates im; MUL multiplies by the bound H with
 // real DC and last-bin products; BANDPASS zeroes bins outside [lo, hi].
+__device__ __forceinline__ cf mul_bin(const PipeOp& op, int k, cf v) {
+    if (k >= op.m) return v;
+    const float hr = __ldg(op.hr + k);
+    if (k == 0 || k == op.m - 1) return cf{v.x * hr, 0.f};
+    const float hi = __ldg(op.hi_ + k);
+    return cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
+}
+
+__device__ __forceinline__ cf apply_op(const PipeOp& op, int k, cf v) {
+    if (op.code == OP_CONJ) return cf{v.x, -v.y};
+    if (op.code == OP_MUL) return mul_bin(op, k, v);
+    if (op.code == OP_BANDPASS && (k < op.lo || k > op.hi)) return cf{0.f, 0.f};
+    return v;
+}
+
+// Every op in order.  The loop bound is a compile-time constant and each op
+// is guarded (no early exit), so the loop unrolls with static accesses.
 __device__ __forceinline__ cf apply_pipe_ops(const RealArgs& a, int k, cf v) {
 #pragma unroll
-    for (int o = 0; o < kMaxOps; o++) {
-        if (o >= a.nops) break;
-        const PipeOp& op = a.ops[o];
-        if (op.code == OP_CONJ) {
-            v.y = -v.y;
-        } else if (op.code == OP_MUL) {
-            if (k < op.m) {
-                const float hr = __ldg(op.hr + k);
-                if (k == 0 || k == op.m - 1) {
-                    v = cf{v.x * hr, 0.f};
-                } else {
-                    const float hi = __ldg(op.hi_ + k);
-                    v = cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
-                }
-            }
-        } else if (op.code == OP_BANDPASS) {
-            if (k < op.lo || k > op.hi) v = cf{0.f, 0.f};
-        }
-    }
+    for (int o = 0; o < kMaxOps; o++)
+        if (o < a.nops) v = apply_op(a.ops[o], k, v);
     return v;
+}
+
+// The op program as a functor for the bin-pair passes: any program, or the
+// common single MUL by a bound spectrum, which skips the op dispatch.
+struct OpsAny {
+    const RealArgs* a;
+    __device__ __forceinline__ cf operator()(int k, cf v) const { return apply_pipe_ops(*a, k, v); }
+};
+struct OpsMul1 {
+    const PipeOp* op;
+    __device__ __forceinline__ cf operator()(int k, cf v) const { return mul_bin(*op, k, v); }
+};
+__host__ __device__ inline bool ops_single_mul(const RealArgs& a) {
+    return a.nops == 1 && a.ops[0].code == OP_MUL;
 }
 
 }  // namespace fafk

@@ -8,28 +8,29 @@ namespace fafk {
 // (reference src/faf_pipeline.c:10-90 + src/chirp.c:421-471)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ cf apply_ops(const RealArgs& a, int k, cf v) {
-#pragma unroll
-    for (int o = 0; o < kMaxOps; o++) {
-        if (o >= a.nops) break;
-        const PipeOp& op = a.ops[o];
-        if (op.code == OP_CONJ) {
-            v.y = -v.y;
-        } else if (op.code == OP_MUL) {
-            if (k < op.m) {
-                const float hr = __ldg(op.hr + k);
-                if (k == 0 || k == op.m - 1) {
-                    v = cf{v.x * hr, 0.f};
-                } else {
-                    const float hi = __ldg(op.hi_ + k);
-                    v = cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
-                }
-            }
-        } else if (op.code == OP_BANDPASS) {
-            if (k < op.lo || k > op.hi) v = cf{0.f, 0.f};
+// Per bin pair: post-pass -> ops -> pre-pass, entirely in registers.
+template <class Ops>
+__device__ __forceinline__ void pipe_pairs(int t, int T, int nc, const SmemIO& mid,
+                                           const float2* __restrict__ stw, const Ops& ops) {
+    for (int k = t; k <= nc / 2; k += T) {
+        if (k == 0) {
+            const cf z = mid.get(0);
+            const cf x0 = ops(0, cf{z.x + z.y, 0.f});
+            const cf xn = ops(nc, cf{z.x - z.y, 0.f});
+            mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
+        } else {
+            const float2 w = __ldg(&stw[k - 1]);
+            cf Xk, Xnk;
+            r2c_pair(mid.get(k), mid.get(nc - k), w, Xk, Xnk);
+            if (k == nc - k) Xk = Xnk;
+            Xk = ops(k, Xk);
+            Xnk = (k == nc - k) ? Xk : ops(nc - k, Xnk);
+            cf Zk, Znk;
+            c2r_pair(Xk, Xnk, w, Zk, Znk);
+            if (k != nc - k) mid.put(k, Zk);
+            mid.put(nc - k, Znk);
         }
     }
-    return v;
 }
 
 template <int E>
@@ -44,26 +45,10 @@ __global__ void __launch_bounds__(1024) k_pipeline(const Shape S, const float2* 
     const SmemIO mid{q.re, q.im};
     run_fft<E>(S, q.t, q.re, q.im, tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid);
     __syncthreads();
-    // Per bin pair: post-pass -> ops -> pre-pass, entirely in registers.
-    for (int k = q.t; k <= nc / 2; k += S.T) {
-        if (k == 0) {
-            const cf z = mid.get(0);
-            cf x0 = apply_ops(a, 0, cf{z.x + z.y, 0.f});
-            cf xn = apply_ops(a, nc, cf{z.x - z.y, 0.f});
-            mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
-        } else {
-            const float2 w = __ldg(&a.stw[k - 1]);
-            cf Xk, Xnk;
-            r2c_pair(mid.get(k), mid.get(nc - k), w, Xk, Xnk);
-            if (k == nc - k) Xk = Xnk;
-            Xk = apply_ops(a, k, Xk);
-            Xnk = (k == nc - k) ? Xk : apply_ops(a, nc - k, Xnk);
-            cf Zk, Znk;
-            c2r_pair(Xk, Xnk, w, Zk, Znk);
-            if (k != nc - k) mid.put(k, Zk);
-            mid.put(nc - k, Znk);
-        }
-    }
+    if (ops_single_mul(a))
+        pipe_pairs(q.t, S.T, nc, mid, a.stw, OpsMul1{&a.ops[0]});
+    else
+        pipe_pairs(q.t, S.T, nc, mid, a.stw, OpsAny{&a});
     __syncthreads();
     RealPairSink snk{a.out_a + bi * a.out_dist, a.scale, live, vec};
     run_fft<E>(S, q.t, q.re, q.im, tw, SmemConjSrc{q.re, q.im}, snk);

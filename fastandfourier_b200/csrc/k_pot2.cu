@@ -184,28 +184,31 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
     }
 }
 
-__device__ __forceinline__ cf apply_ops2(const RealArgs& a, int k, cf v) {
-#pragma unroll
-    for (int o = 0; o < kMaxOps; o++) {
-        if (o >= a.nops) break;
-        const PipeOp& op = a.ops[o];
-        if (op.code == OP_CONJ) {
-            v.y = -v.y;
-        } else if (op.code == OP_MUL) {
-            if (k < op.m) {
-                const float hr = __ldg(op.hr + k);
-                if (k == 0 || k == op.m - 1) {
-                    v = cf{v.x * hr, 0.f};
-                } else {
-                    const float hi = __ldg(op.hi_ + k);
-                    v = cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
-                }
-            }
-        } else if (op.code == OP_BANDPASS) {
-            if (k < op.lo || k > op.hi) v = cf{0.f, 0.f};
+// Per bin pair of the pipeline: post-pass -> ops -> pre-pass, in registers,
+// in place on the workspace.
+template <int N, class Ops>
+__device__ __forceinline__ void pipe_middle(int t, const SmemC& mid,
+                                            const float2* __restrict__ stw, const Ops& ops) {
+    constexpr int nc = N, T = P2<N>::T;
+    for (int k = t; k <= nc / 2; k += T) {
+        if (k == 0) {
+            const cf z = mid.get(0);
+            const cf x0 = ops(0, cf{z.x + z.y, 0.f});
+            const cf xn = ops(nc, cf{z.x - z.y, 0.f});
+            mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
+        } else {
+            const float2 w = __ldg(&stw[k - 1]);
+            cf Xk, Xnk;
+            r2c_pair(mid.get(k), mid.get(nc - k), w, Xk, Xnk);
+            if (k == nc - k) Xk = Xnk;
+            Xk = ops(k, Xk);
+            Xnk = (k == nc - k) ? Xk : ops(nc - k, Xnk);
+            cf Zk, Znk;
+            c2r_pair(Xk, Xnk, w, Zk, Znk);
+            if (k != nc - k) mid.put(k, Zk);
+            mid.put(nc - k, Znk);
         }
     }
-    return v;
 }
 
 template <int N, bool ASYNC>
@@ -234,26 +237,10 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
                               mid, q.sync);
         }
         q.sync();
-        // Per bin pair: post-pass -> ops -> pre-pass, in registers.
-        for (int k = q.t; k <= nc / 2; k += T) {
-            if (k == 0) {
-                const cf z = mid.get(0);
-                const cf x0 = apply_ops2(a, 0, cf{z.x + z.y, 0.f});
-                const cf xn = apply_ops2(a, nc, cf{z.x - z.y, 0.f});
-                mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
-            } else {
-                const float2 w = __ldg(&a.stw[k - 1]);
-                cf Xk, Xnk;
-                r2c_pair(mid.get(k), mid.get(nc - k), w, Xk, Xnk);
-                if (k == nc - k) Xk = Xnk;
-                Xk = apply_ops2(a, k, Xk);
-                Xnk = (k == nc - k) ? Xk : apply_ops2(a, nc - k, Xnk);
-                cf Zk, Znk;
-                c2r_pair(Xk, Xnk, w, Zk, Znk);
-                if (k != nc - k) mid.put(k, Zk);
-                mid.put(nc - k, Znk);
-            }
-        }
+        if (ops_single_mul(a))
+            pipe_middle<N>(q.t, mid, a.stw, OpsMul1{&a.ops[0]});
+        else
+            pipe_middle<N>(q.t, mid, a.stw, OpsAny{&a});
         q.sync();
         ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
                           RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec}, q.sync);
