@@ -21,7 +21,8 @@ from ._lib import (B_CUDA, DIR_FORWARD, DIR_INVERSE, FLAG_BLUESTEIN, FLAG_MEASUR
                    T_STFT)
 
 __all__ = ["FafError", "Transform", "Uneven", "Server", "Request", "config", "lib", "available",
-           "B_CUDA", "DIR_FORWARD", "DIR_INVERSE", "FLAG_TENSOR_CORE", "FLAG_BLUESTEIN", "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
+           "B_CUDA", "DIR_FORWARD", "DIR_INVERSE", "FLAG_TENSOR_CORE", "FLAG_BLUESTEIN",
+           "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
            "L_INTERLEAVED", "L_REAL", "L_SPLIT", "N_DEFAULT", "N_FORWARD", "N_NONE", "N_ORTHO",
            "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
 
@@ -249,6 +250,12 @@ class Transform:
         return cls(C.lib().faf_create_stft(ctypes.byref(c)))
 
     @classmethod
+    def istft(cls, n, *, win=0, hop=0):
+        """Inverse STFT (faf_cuda_create_istft): frames -> signal."""
+        c = config(n, hop=hop, win=win)
+        return cls(C.lib().faf_cuda_create_istft(ctypes.byref(c)))
+
+    @classmethod
     def chirp(cls, source):
         return cls(C.lib().chirp_compile(source.encode()))
 
@@ -369,6 +376,18 @@ class Transform:
         self.execute_batched(_buf(out_re, out_im, F * nb, L_HERMITIAN),
                              _buf(x, None, L, L_REAL), n_sig)
         return out_re, out_im
+
+    def istft_frames(self, Xr, Xi, out=None):
+        """Inverse STFT of frames (n_sig, F, n/2+1) -> (n_sig, (F-1) hop + win)."""
+        nb = self.n // 2 + 1
+        F = Xr.shape[-2]
+        L = (F - 1) * self.s.hop_length + self.s.win_length
+        n_sig = (Xr.numel() if hasattr(Xr, "numel") else Xr.size) // (F * nb)
+        if out is None:
+            out = _empty_like_batch(Xr, tuple(Xr.shape[:-2]) + (L,))
+        self.execute_batched(_buf(out, None, L, L_REAL), _buf(Xr, Xi, F * nb, L_HERMITIAN),
+                             n_sig)
+        return out
 
     def close(self):
         if self._p:

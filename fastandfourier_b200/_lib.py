@@ -127,6 +127,7 @@ _SIGS = [
     ("faf_cuda_plan_kind", ctypes.c_char_p, [TP]),
     ("faf_cuda_last_launches", ctypes.c_int, []),
     ("faf_cuda_tc_status", ctypes.c_int, [TP]),
+    ("faf_cuda_create_istft", TP, [ctypes.POINTER(faf_config)]),
     ("faf_cuda_set_stream", ctypes.c_int, [TP, ctypes.c_void_p]),
     ("faf_cuda_get_stream", ctypes.c_void_p, [TP]),
     ("faf_cuda_synchronize", ctypes.c_int, [TP]),

@@ -569,7 +569,7 @@ int resolve_pipeline_ops(const faf_transform* t, fafk::PipeOp* ops, int cap, boo
                 // Host H: copied to a plan buffer on every execute (H is read
                 // live, like the reference, so later edits are honoured).
                 fafp::DevicePlan* p = plan_of(t);
-                std::lock_guard<std::mutex> lk(p->mu);
+                std::lock_guard<std::mutex> lk(p->scratch_mu);
                 const size_t bytes = 2 * nb * sizeof(float);
                 if (p->scratch_bytes < bytes) {
                     cudaFree(p->d_scratch);

@@ -510,6 +510,46 @@ extern "C" faf_transform* faf_create(faf_transform_type type, const faf_config* 
     }
 }
 
+extern "C" faf_transform* faf_cuda_create_istft(const faf_config* cfg) {
+    if (!cfg) {
+        fail("faf_cuda_create_istft: cfg is NULL");
+        return nullptr;
+    }
+    faf_config c = *cfg;
+    if (c.win_length == 0) c.win_length = c.n;
+    if (c.hop_length == 0) c.hop_length = c.win_length / 4;
+    if (c.win_length > c.n || c.hop_length == 0 || c.hop_length > c.win_length) {
+        fail("inverse STFT needs 0 < hop <= win <= n (n=%zu, win=%zu, hop=%zu)", c.n,
+             c.win_length, c.hop_length);
+        return nullptr;
+    }
+    if (c.n < 2 || c.n % 2 || !is_5_smooth(c.n)) {
+        fail("inverse STFT needs an even 5-smooth FFT size, got %zu", c.n);
+        return nullptr;
+    }
+    if (!backend_ok(c)) return nullptr;
+    faf_transform* t = alloc_transform();
+    if (!t) return nullptr;
+    t->type = FAF_TRANSFORM_STFT;
+    c.dir = FAF_DIR_INVERSE;
+    c.layout = FAF_LAYOUT_HERMITIAN;
+    c.norm = FAF_NORM_NONE;
+    if (c.backend == FAF_BACKEND_AUTO) c.backend = FAF_BACKEND_CUDA;
+    apply_resolved(t, c);
+    t->flags |= FAF_FLAG_INVERSE;
+    t->hop_length = c.hop_length;
+    t->win_length = c.win_length;
+    std::string err;
+    DevicePlan* p = fafp::plan_istft((int)c.n, (int)c.win_length, (int)c.hop_length, err);
+    if (!p) {
+        fail("CUDA plan for inverse STFT n=%zu: %s", c.n, err.c_str());
+        faf_destroy_transform(t);
+        return nullptr;
+    }
+    t->device_plan = p;
+    return t;
+}
+
 extern "C" faf_transform* faf_create_inverse(const faf_transform* fwd) {
     if (!fwd) {
         fail("faf_create_inverse: transform is NULL");

@@ -134,9 +134,39 @@ int check_pipeline(const faf_transform* t, const faf_buffer* out, const faf_buff
     return 0;
 }
 
+// Inverse STFT (faf_cuda_create_istft): HERMITIAN frames F x (n/2+1) in,
+// REAL signal of (F - 1) hop + win samples out.
+int check_istft(const faf_transform* t, const faf_buffer* out, const faf_buffer* in,
+                Request& r) {
+    const size_t n = t->n, nb = n / 2 + 1, win = t->win_length, hop = t->hop_length;
+    if (in->layout != FAF_LAYOUT_HERMITIAN || !in->re || !in->im)
+        return fail("inverse STFT input must be HERMITIAN split frames (re and im)");
+    if (in->n == 0 || in->n % nb)
+        return fail("inverse STFT input n=%zu is not a whole number of %zu-bin frames", in->n, nb);
+    const size_t F = in->n / nb, L = (F - 1) * hop + win;
+    if (out->layout != FAF_LAYOUT_REAL || !out->re)
+        return fail("inverse STFT output must be REAL");
+    if (out->n != L)
+        return fail("inverse STFT output n=%zu, expected (%zu - 1) * %zu + %zu = %zu", out->n, F,
+                    hop, win, L);
+    r.framed = true;
+    r.frames = (long long)F;
+    r.sig_len = (long long)L;
+    r.in_a = (const float*)in->re;
+    r.in_b = (const float*)in->im;
+    r.out_a = (float*)out->re;
+    r.in_len = in->n;
+    r.out_len = L;
+    return 0;
+}
+
 int check_stft(const faf_transform* t, const faf_buffer* out, const faf_buffer* in,
                Request& r) {
     if (!in->re || !out->re) return fail("execute buffers must provide re");
+    {
+        DevicePlan* p = plan_of(t);
+        if (p && p->kind == Kind::ISTFT) return check_istft(t, out, in, r);
+    }
     const size_t n = t->n, nb = n / 2 + 1, win = t->win_length, hop = t->hop_length;
     if (in->layout == FAF_LAYOUT_REAL) {
         // Framed real STFT: F = 1 + (L - win) / hop frames of n/2+1 bins.
@@ -428,7 +458,14 @@ int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t s
         break;
     }
     case FAF_TRANSFORM_STFT:
-        if (r.framed) {
+        if (p->kind == Kind::ISTFT) {
+            if (r.batch > 1 && r.in_dist != (long long)r.in_len)
+                return fail("batched inverse STFT frames must be packed");
+            if (r.batch > 1 && r.out_dist != (long long)r.out_len)
+                return fail("batched inverse STFT output must be packed");
+            e = fafp::exec_istft(p, r.in_a, r.in_b, r.out_a, r.batch, r.frames, r.sig_len, st);
+            launches = 2;
+        } else if (r.framed) {
             DevicePlan* fp = plan_of(t->inner);
             const long long sig_dist = r.in_dist ? r.in_dist : r.sig_len;
             if (r.batch > 1 && sig_dist != r.sig_len)
@@ -560,6 +597,7 @@ extern "C" const char* faf_cuda_plan_kind(const faf_transform* t) {
     case Kind::C2R: return "c2r";
     case Kind::PIPELINE: return "pipeline";
     case Kind::STFT: return "stft";
+    case Kind::ISTFT: return "istft";
     }
     return "unknown";
 }

@@ -146,6 +146,10 @@ int large_pot2_launches(int n1, int n2, long long batch);
 cudaError_t large_pot2_prepare(int n1, int n2);  // kernel attributes, before any capture
 cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st);
 
+// Overlap-add of the inverse STFT (k_istft.cu).
+cudaError_t launch_ola(const float* tmp, const float* w, int n, int win, int hop, long long F,
+                       long long L, float* y, long long n_sig, cudaStream_t st);
+
 // Tensor-core precision form of the power-of-two C2C (k_tc.cu).
 bool tc_supported(int log2n);
 cudaError_t prepare_c2c_tc(int log2n);  // kernel attributes, before any capture

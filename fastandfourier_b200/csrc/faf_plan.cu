@@ -582,6 +582,29 @@ DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err) {
     return p;
 }
 
+// Inverse STFT: the C2R of n (1/n scaled, so irfft(rfft(x)) = x) plus the
+// same symmetric Hann window the forward STFT applies.
+DevicePlan* plan_istft(int n, int win, int hop, std::string& err) {
+    if (needs_four_step(n / 2)) {
+        err = "STFT frames of " + std::to_string(n) + " samples exceed one CTA";
+        return nullptr;
+    }
+    DevicePlan* p = plan_r2c(n, true, (float)(1.0 / (double)n), err);
+    if (!p) return nullptr;
+    p->kind = Kind::ISTFT;
+    p->win = win;
+    p->hop = hop;
+    std::vector<float> w(std::max(n, 1), 0.0f);
+    for (int i = 0; i < win; i++)
+        w[i] = win > 1 ? (float)(0.5 * (1.0 - std::cos(2.0 * M_PI * (double)i / (double)(win - 1))))
+                       : 1.0f;
+    if (!cuda_ok(upload(&p->d_window, w.data(), w.size()), err, "window upload")) {
+        plan_free(p);
+        return nullptr;
+    }
+    return p;
+}
+
 // ---------------------------------------------------------------------------
 // Device-pointer execution
 // ---------------------------------------------------------------------------
@@ -623,7 +646,7 @@ static cudaError_t run_large(DevicePlan* p, int kind, const void* args, long lon
     a.cta_floats = (kind == 0 ? 2LL : 4LL) * p->n1 * p->n2;
     const size_t bytes = (size_t)grid * (size_t)a.cta_floats * sizeof(float);
     {
-        std::lock_guard<std::mutex> lk(p->mu);
+        std::lock_guard<std::mutex> lk(p->scratch_mu);
         if (p->work_bytes < bytes) {
             cudaFree(p->d_work);
             p->d_work = nullptr;
@@ -647,7 +670,7 @@ static cudaError_t run_large_pot2(DevicePlan* p, const float* in_re, const float
     const long long chunk = std::min(batch, fafk::large_pot2_chunk(n));
     const size_t bytes = (size_t)chunk * 2 * (size_t)n * sizeof(float);
     {
-        std::lock_guard<std::mutex> lk(p->mu);
+        std::lock_guard<std::mutex> lk(p->scratch_mu);
         if (p->work_bytes < bytes) {
             cudaFree(p->d_work);
             p->d_work = nullptr;
@@ -802,6 +825,29 @@ cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long 
                                  geometry_ct(p->inner, slots, batch), st);
     return fafk::launch_stft(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                              p->inner.d_tw, a, st);
+}
+
+cudaError_t exec_istft(DevicePlan* p, const float* Xr, const float* Xi, float* y, long long n_sig,
+                       long long frames, long long sig_len, cudaStream_t st) {
+    const long long nb = p->n / 2 + 1;
+    const size_t bytes = (size_t)(n_sig * frames) * (size_t)p->n * sizeof(float);
+    float* tmp = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(p->scratch_mu);
+        if (p->scratch_bytes < bytes) {
+            cudaFree(p->d_scratch);
+            p->d_scratch = nullptr;
+            p->scratch_bytes = 0;
+            cudaError_t e = cudaMalloc(&p->d_scratch, bytes);
+            if (e != cudaSuccess) return e;
+            p->scratch_bytes = bytes;
+        }
+        tmp = (float*)p->d_scratch;
+    }
+    cudaError_t e = exec_c2r(p, Xr, Xi, tmp, n_sig * frames, nb, p->n, false, st);
+    if (e != cudaSuccess) return e;
+    return fafk::launch_ola(tmp, p->d_window, p->n, p->win, p->hop, frames, sig_len, y, n_sig,
+                            st);
 }
 
 }  // namespace fafp

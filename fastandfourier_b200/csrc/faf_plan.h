@@ -51,7 +51,8 @@ enum class Kind {
     R2C,
     C2R,
     PIPELINE,   // fused R2C -> ops -> C2R
-    STFT        // framed, windowed R2C
+    STFT,       // framed, windowed R2C
+    ISTFT       // batched C2R of frames -> windowed overlap-add
 };
 
 struct DevicePlan {
@@ -85,8 +86,11 @@ struct DevicePlan {
     // launch state
     cudaStream_t stream = nullptr;  // 0 = legacy default stream
     bool user_stream = false;
-    // staging for host buffers and four-step scratch
+    // staging for host buffers (mu, held by a host-buffer execute from copy-in
+    // to copy-out) and device scratch grown by the kernels' launchers
+    // (scratch_mu, taken inside that execute, so it must be another mutex)
     std::mutex mu;
+    std::mutex scratch_mu;
     void* d_stage = nullptr;
     size_t stage_bytes = 0;
     // chunked host-buffer path: copy streams and per-slot events (lazy)
@@ -100,6 +104,7 @@ DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::stri
 DevicePlan* plan_r2c(int n, bool inverse, float scale, std::string& err);
 DevicePlan* plan_pipeline(int n, float scale_fwd, float scale_inv, std::string& err);
 DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err);
+DevicePlan* plan_istft(int n, int win, int hop, std::string& err);
 void plan_free(DevicePlan* p);
 
 // Device-pointer executes (enqueue on `st`).
@@ -115,6 +120,8 @@ cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long bat
                           int nops, cudaStream_t st);
 cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long long n_sig,
                       long long sig_len, long long frames, bool interleaved, cudaStream_t st);
+cudaError_t exec_istft(DevicePlan* p, const float* Xr, const float* Xi, float* y, long long n_sig,
+                       long long frames, long long sig_len, cudaStream_t st);
 
 // Four-step tables of p for complex length n (n1, n2, f1, f2, t1, t2, twiddles).
 bool build_large(DevicePlan* p, int n, std::string& err);

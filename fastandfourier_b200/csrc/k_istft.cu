@@ -1,0 +1,46 @@
+// k_istft.cu -- overlap-add of the inverse STFT (no counterpart in the
+// reference, whose faf_create_inverse of an STFT returns another forward
+// STFT, src/faf_core.c:1122-1123).
+//
+// The frames have already been through the batched C2R (1/n scaled) into
+// tmp[(s F + f) n + j]; output sample t of signal s is the weighted
+// overlap-add of every frame f with f hop <= t < f hop + win:
+//     y[t] = sum_f w[t - f hop] tmp_f[t - f hop] / sum_f w[t - f hop]^2
+// and 0 where that window envelope is below 1e-10 (the ends of a symmetric
+// Hann window, w[0] = 0).  One thread per output sample sums its frames in
+// frame order, so the result does not depend on the launch.
+#include <algorithm>
+
+#include "faf_kernels_common.cuh"
+
+namespace fafk {
+
+__global__ void k_ola(const float* __restrict__ tmp, const float* __restrict__ w, int n, int win,
+                      int hop, long long F, long long L, float* __restrict__ y, long long n_sig) {
+    const long long total = n_sig * L;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long s = idx / L, t = idx - s * L;
+        const long long f_hi = min(F - 1, t / hop);
+        const long long f_lo = t >= win ? (t - win) / hop + 1 : 0;
+        float sum = 0.f, env = 0.f;
+        for (long long f = f_lo; f <= f_hi; f++) {
+            const int j = (int)(t - f * hop);
+            const float wj = __ldg(&w[j]);
+            sum = fmaf(wj, __ldg(&tmp[(s * F + f) * n + j]), sum);
+            env = fmaf(wj, wj, env);
+        }
+        y[idx] = env > 1e-10f ? sum / env : 0.f;
+    }
+}
+
+cudaError_t launch_ola(const float* tmp, const float* w, int n, int win, int hop, long long F,
+                       long long L, float* y, long long n_sig, cudaStream_t st) {
+    const long long total = n_sig * L;
+    if (total <= 0) return cudaSuccess;
+    const long long blocks = std::min<long long>((total + 255) / 256, 148LL * 16);
+    k_ola<<<(unsigned)blocks, 256, 0, st>>>(tmp, w, n, win, hop, F, L, y, n_sig);
+    return cudaGetLastError();
+}
+
+}  // namespace fafk

@@ -64,6 +64,18 @@ int faf_cuda_synchronize(const faf_transform *t);
 int faf_execute_batched(const faf_transform *t, faf_buffer *out, const faf_buffer *in,
                         size_t batch, size_t in_dist, size_t out_dist);
 
+/* ---- inverse STFT ----------------------------------------------------------- */
+
+/* No counterpart in the reference (its faf_create_inverse of an STFT returns
+ * another forward STFT, src/faf_core.c:1122).  cfg: n (even, 5-smooth),
+ * win_length (default n), hop_length (default win/4), 0 < hop <= win <= n.
+ * faf_execute / faf_execute_batched take HERMITIAN split frames F x (n/2+1)
+ * and write a REAL signal of (F - 1) * hop + win samples: each frame's
+ * inverse real FFT (1/n scaled) times the same symmetric Hann window as the
+ * forward STFT, overlap-added and divided by the summed squared window
+ * (0 where that sum is below 1e-10).  Batched signals must be packed. */
+faf_transform *faf_cuda_create_istft(const faf_config *cfg);
+
 /* ---- uneven batches (one persistent launch) ------------------------------- */
 
 typedef struct faf_uneven faf_uneven;

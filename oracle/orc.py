@@ -133,6 +133,28 @@ def stft(x, n, win, hop):
     return Xr, Xi
 
 
+def istft(Xr, Xi, n, win, hop):
+    """Inverse STFT by weighted overlap-add, in FP64 (the reference has no
+    inverse STFT: its faf_create_inverse of an STFT returns a forward STFT,
+    src/faf_core.c:1122-1123).  Frames (n_sig, F, n//2+1) -> signals
+    (n_sig, (F-1) hop + win): irfft of each frame, times the symmetric Hann
+    window of the forward STFT (src/faf_twiddles.c:159-163), overlap-added and
+    divided by the summed squared window (0 where it is below 1e-10)."""
+    X = np.asarray(Xr, np.float64) + 1j * np.asarray(Xi, np.float64)
+    X = X.reshape((-1,) + X.shape[-2:])
+    n_sig, F, _ = X.shape
+    frames = np.fft.irfft(X, n=n, axis=-1)[..., :win]
+    i = np.arange(win)
+    w = 0.5 * (1 - np.cos(2 * np.pi * i / (win - 1))) if win > 1 else np.ones(1)
+    L = (F - 1) * hop + win
+    y = np.zeros((n_sig, L))
+    env = np.zeros(L)
+    for f in range(F):
+        y[:, f * hop:f * hop + win] += w * frames[:, f]
+        env[f * hop:f * hop + win] += w * w
+    return np.where(env > 1e-10, y / np.where(env > 1e-10, env, 1.0), 0.0)
+
+
 def hann(n):
     w = np.empty(n, np.float32)
     lib().orc_hann(_p(w), n)

@@ -401,3 +401,28 @@ def test_host_buffers_chunked_overlap(cuda):
     sr, si = s.stft_frames(xs)
     dr2, di2 = s.stft_frames(torch.from_numpy(xs).cuda())
     assert np.array_equal(sr, dr2.cpu().numpy()) and np.array_equal(si, di2.cpu().numpy())
+
+
+def test_host_buffers_on_four_step_and_host_mask(cuda):
+    """Host buffers through the paths that grow device scratch inside the
+    execute (four-step scratch, a host-bound spectrum): results equal the
+    device-buffer path."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    rng = seeded(616)
+    re = rng.uniform(-1, 1, (3, 32768)).astype(np.float32)
+    im = rng.uniform(-1, 1, (3, 32768)).astype(np.float32)
+    c = F.Transform.fft(32768)
+    hr, hi = c.c2c(re, im)
+    dr, di = c.c2c(torch.from_numpy(re).cuda(), torch.from_numpy(im).cuda())
+    assert np.array_equal(hr, dr.cpu().numpy()) and np.array_equal(hi, di.cpu().numpy())
+    x = rng.standard_normal((2, 65536)).astype(np.float32)
+    r = F.Transform.rfft(65536)
+    Xr, Xi = r.r2c(x)
+    assert orc.rel_l2_complex(Xr, Xi, orc.fp64_r2c(x)) <= REL_L2_TOL
+    m = np.linspace(0, 1, 2049).astype(np.float32)
+    p = F.Transform.chirp("(pipeline (rfft :size 4096) (mul-spectrum) (irfft))")
+    p.bind(m, np.zeros_like(m), 2049)  # host H, host signal
+    xs = rng.standard_normal((5, 4096)).astype(np.float32)
+    y = p.pipeline(xs)
+    assert orc.rel_l2(y, orc.pipeline(xs, [(orc.OP_MUL, 0, 0)], m, np.zeros_like(m))) <= REL_L2_TOL
