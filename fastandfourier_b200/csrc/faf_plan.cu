@@ -277,7 +277,8 @@ static bool stage_ok(const float* x, long long dist) {
     return ((unsigned long long)(size_t)x % 16 == 0) && (dist % 4 == 0);
 }
 
-// FAF_CUDA_STAGING=1 turns input staging on for kernels that default to off.
+// FAF_CUDA_STAGING=1 turns input staging on (the R2C and pipeline kernels
+// default to off).
 static bool stage_env() {
     const char* env = std::getenv("FAF_CUDA_STAGING");
     return env && env[0] == '1';
@@ -763,9 +764,13 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
         return run_large(p, 1, &a, batch, st);
     }
     const int slots = p->inner.n + 1;
+    // measured on B200 (n = 4096, batch 8192): 1024-thread CTAs without
+    // input staging beat staged 512-thread CTAs (2900 vs 2580 GB/s)
     if (p->inner.ct_log2)
         return fafk::launch_pot2(1, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch, stage_ok(x, in_dist)), st);
+                                 geometry_ct(p->inner, slots, batch,
+                                             stage_env() && stage_ok(x, in_dist), 1024),
+                                 st);
     return fafk::launch_r2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);
 }
@@ -802,10 +807,11 @@ cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long bat
     }
     const int slots = p->inner.n + 1;
     if (p->inner.ct_log2)
-        // measured on B200 (n = 4096): the two-FFT pipeline runs best without
-        // input staging at ~256 threads per CTA
+        // measured on B200 (n = 4096, batch 8192): the two-FFT pipeline runs
+        // best without input staging in 1024-thread CTAs (1816 GB/s against
+        // 1699 at 512 and 1686 at 256)
         return fafk::launch_pot2(3, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch, stage_env(), 256), st);
+                                 geometry_ct(p->inner, slots, batch, stage_env(), 1024), st);
     return fafk::launch_pipeline(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                                  p->inner.d_tw, a, st);
 }
