@@ -26,6 +26,8 @@ FLAG_INVERSE, FLAG_REAL = 0x1, 0x8
 FLAG_BLUESTEIN, FLAG_MEASURE = 1 << 12, 1 << 13
 FLAG_TENSOR_CORE = 1 << 16
 CHIRP_OP_CONJ, CHIRP_OP_MUL, CHIRP_OP_BANDPASS = 0x7FFFFFFD, 0x7FFFFFFE, 0x7FFFFFFF
+(CHIRP_DEVICE_GAIN, CHIRP_DEVICE_PHASE, CHIRP_DEVICE_DELAY, CHIRP_DEVICE_LOWPASS,
+ CHIRP_DEVICE_HIGHPASS) = range(5)
 FAF_CALL_BUILTIN = 30
 
 
@@ -160,7 +162,11 @@ _SIGS = [
     ("chirp_bind", ctypes.c_int, [TP, ctypes.c_char_p, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.c_size_t]),
     ("chirp_register_spectral", ctypes.c_int, [ctypes.c_char_p, SPECTRAL_FN, ctypes.c_void_p]),
+    ("chirp_register_spectral_device", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int,
+                                                      ctypes.c_double]),
     ("chirp_cleanup", None, []),
+    ("chirp_apply_split_f32", None, [TP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     ("chirp_count", ctypes.c_int, []),
     ("faf_herm_mul_f32", None, [ctypes.c_void_p] * 6 + [ctypes.c_size_t]),
     ("faf_herm_mul_conj_f32", None, [ctypes.c_void_p] * 6 + [ctypes.c_size_t]),

@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <cmath>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -34,7 +35,19 @@ struct Builtin {
     chirp_spectral_fn_f64 f64 = nullptr;
     int kind = CHIRP_KIND_SPECTRAL;
     void* ctx = nullptr;
+    bool device = false;  // chirp_register_spectral_device: runs in the fused kernel
+    int dop = 0;          // chirp_device_op
+    double p0 = 0;
 };
+
+// Phase of the circular delay at bin k of an n-point transform: -2 pi
+// (k d mod n) / n, reduced in FP64 as the kernel does.
+void delay_phase(size_t k, double d, size_t n, double* c, double* s) {
+    const double r = std::fmod((double)k * d, (double)n);
+    const double a = -2.0 * M_PI * r / (double)n;
+    *c = std::cos(a);
+    *s = std::sin(a);
+}
 
 std::mutex g_reg_mu;
 std::vector<Builtin> g_reg;
@@ -396,6 +409,38 @@ extern "C" int chirp_register_spectral_ex(const char* name, chirp_spectral_fn f3
     g_reg[idx].f64 = f64;
     g_reg[idx].kind = CHIRP_KIND_SPECTRAL;
     g_reg[idx].ctx = ctx;
+    g_reg[idx].device = false;
+    return idx;
+}
+
+extern "C" int chirp_register_spectral_device(const char* name, chirp_device_op op, double p0) {
+    if (!name || !*name) {
+        fail("chirp_register_spectral_device: name is required");
+        return -1;
+    }
+    if ((int)op < CHIRP_DEVICE_GAIN || (int)op > CHIRP_DEVICE_HIGHPASS) {
+        fail("chirp_register_spectral_device: unknown op %d", (int)op);
+        return -1;
+    }
+    if (!std::isfinite(p0) || ((op == CHIRP_DEVICE_LOWPASS || op == CHIRP_DEVICE_HIGHPASS) && p0 < 0)) {
+        fail("chirp_register_spectral_device: bad parameter %g for op %d", p0, (int)op);
+        return -1;
+    }
+    std::lock_guard<std::mutex> lk(g_reg_mu);
+    int idx = lookup(name);
+    if (idx < 0) {
+        g_reg.push_back(Builtin());
+        idx = (int)g_reg.size() - 1;
+        g_reg[idx].name = name;
+    }
+    Builtin& b = g_reg[idx];
+    b.f32 = nullptr;
+    b.f64 = nullptr;
+    b.ctx = nullptr;
+    b.kind = CHIRP_KIND_SPECTRAL;
+    b.device = true;
+    b.dop = (int)op;
+    b.p0 = p0;
     return idx;
 }
 
@@ -478,6 +523,22 @@ extern "C" void chirp_apply_split_f32(const faf_transform* t, uint32_t a0, uint3
         std::lock_guard<std::mutex> lk(g_reg_mu);
         if ((int)a0 < 0 || a0 >= g_reg.size()) return;
         b = g_reg[a0];
+    }
+    if (b.device) {  // the device op's math, on host bins (FP64 phases)
+        if (!im) return;
+        const size_t len = t ? t->n : 2 * (n - 1);
+        for (size_t k = 0; k < n; k++) {
+            double c = 1, s = 0, g = 1;
+            if (b.dop == CHIRP_DEVICE_GAIN) g = b.p0;
+            else if (b.dop == CHIRP_DEVICE_PHASE) { c = std::cos(b.p0); s = std::sin(b.p0); }
+            else if (b.dop == CHIRP_DEVICE_DELAY) delay_phase(k, b.p0, len, &c, &s);
+            else if (b.dop == CHIRP_DEVICE_LOWPASS) g = (double)k > b.p0 ? 0.0 : 1.0;
+            else if (b.dop == CHIRP_DEVICE_HIGHPASS) g = (double)k < b.p0 ? 0.0 : 1.0;
+            const double r = re[k], i = im[k];
+            re[k] = (float)(g * (r * c - i * s));
+            im[k] = (float)(g * (r * s + i * c));
+        }
+        return;
     }
     if (!b.f32 || !im) return;
     b.f32(re, im, n, b.ctx);
@@ -590,8 +651,41 @@ int resolve_pipeline_ops(const faf_transform* t, fafk::PipeOp* ops, int cap, boo
                 op.hi_ = dh + nb;
             }
         } else {
-            *host_ops = true;  // a registered host callback
-            continue;
+            Builtin b;
+            {
+                std::lock_guard<std::mutex> lk(g_reg_mu);
+                if (in.a0 < g_reg.size()) b = g_reg[in.a0];
+            }
+            if (!b.device) {
+                *host_ops = true;  // a registered host callback
+                continue;
+            }
+            switch (b.dop) {
+            case CHIRP_DEVICE_GAIN:
+                op.code = fafk::OP_SCALE;
+                op.f0 = (float)b.p0;
+                break;
+            case CHIRP_DEVICE_PHASE:
+                op.code = fafk::OP_ROTATE;
+                op.f0 = (float)std::cos(b.p0);
+                op.f1 = (float)std::sin(b.p0);
+                break;
+            case CHIRP_DEVICE_DELAY:
+                op.code = fafk::OP_DELAY;
+                op.d0 = b.p0;
+                op.n = (int)t->n;
+                break;
+            case CHIRP_DEVICE_LOWPASS:
+                op.code = fafk::OP_BANDPASS;
+                op.lo = 0;
+                op.hi = (int)std::min(std::floor(b.p0), 2147483647.0);
+                break;
+            default:  // CHIRP_DEVICE_HIGHPASS
+                op.code = fafk::OP_BANDPASS;
+                op.lo = (int)std::min(std::ceil(b.p0), 2147483647.0);
+                op.hi = 0x7fffffff;
+                break;
+            }
         }
         if (k >= cap) return fail("too many pipeline ops");
         ops[k++] = op;

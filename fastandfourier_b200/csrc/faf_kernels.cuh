@@ -19,7 +19,8 @@ struct Geometry {
 };
 
 // Spectral op codes used inside the fused pipeline kernel.
-enum : int { OP_NONE = 0, OP_CONJ = 1, OP_MUL = 2, OP_BANDPASS = 3 };
+enum : int { OP_NONE = 0, OP_CONJ = 1, OP_MUL = 2, OP_BANDPASS = 3, OP_SCALE = 4,
+              OP_ROTATE = 5, OP_DELAY = 6 };
 constexpr int kMaxOps = 8;
 
 struct PipeOp {
@@ -28,6 +29,9 @@ struct PipeOp {
     int m;               // MUL: bins used = min(bound bins, n/2+1)
     const float* hr;     // MUL: device H planes
     const float* hi_;
+    float f0, f1;        // SCALE: f0; ROTATE: f0 + i f1
+    double d0;           // DELAY: samples of delay
+    int n;               // DELAY: transform length
 };
 
 struct C2CArgs {

@@ -297,10 +297,24 @@ __device__ __forceinline__ cf mul_bin(const PipeOp& op, int k, cf v) {
     return cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
 }
 
+// Device spectral ops (chirp_register_spectral_device): gain, fixed phase,
+// and a circular delay whose phase is reduced in FP64 (k d mod n) before the
+// sine / cosine, so large k d keeps its accuracy.
+__device__ __forceinline__ cf delay_bin(const PipeOp& op, int k, cf v) {
+    const double r = fmod((double)k * op.d0, (double)op.n);
+    double s, c;
+    sincospi(-2.0 * r / (double)op.n, &s, &c);
+    const float fs = (float)s, fc = (float)c;
+    return cf{v.x * fc - v.y * fs, fmaf(v.x, fs, v.y * fc)};
+}
+
 __device__ __forceinline__ cf apply_op(const PipeOp& op, int k, cf v) {
     if (op.code == OP_CONJ) return cf{v.x, -v.y};
     if (op.code == OP_MUL) return mul_bin(op, k, v);
     if (op.code == OP_BANDPASS && (k < op.lo || k > op.hi)) return cf{0.f, 0.f};
+    if (op.code == OP_SCALE) return cf{v.x * op.f0, v.y * op.f0};
+    if (op.code == OP_ROTATE) return cf{v.x * op.f0 - v.y * op.f1, fmaf(v.x, op.f1, v.y * op.f0)};
+    if (op.code == OP_DELAY) return delay_bin(op, k, v);
     return v;
 }
 

@@ -51,6 +51,22 @@ void *chirp_builtin_ctx(int idx);
 const char *chirp_builtin_name(int idx);
 int chirp_count(void);
 
+/* Device spectral ops.  No counterpart in the reference, whose
+ * (spectral NAME) always calls a host function.  A name registered here runs
+ * inside the fused GPU pipeline kernel, with no host round trip; if the same
+ * pipeline also holds a host callback, every op of it runs on the host, this
+ * one included.  Registering a name replaces an earlier host or device
+ * registration of that name; returns its index >= 0, or -1. */
+typedef enum {
+    CHIRP_DEVICE_GAIN = 0,     /* every bin times p0 (real) */
+    CHIRP_DEVICE_PHASE = 1,    /* every bin times exp(i p0), p0 in radians */
+    CHIRP_DEVICE_DELAY = 2,    /* bin k times exp(-2 pi i k p0 / n): circular delay by
+                                  p0 samples (n = the pipeline's length) */
+    CHIRP_DEVICE_LOWPASS = 3,  /* bins k > p0 set to 0 */
+    CHIRP_DEVICE_HIGHPASS = 4  /* bins k < p0 set to 0 */
+} chirp_device_op;
+int chirp_register_spectral_device(const char *name, chirp_device_op op, double p0);
+
 /* Bind the auxiliary spectrum "H" (also "mul-spectrum" / "kernel") used by
  * (mul-spectrum).  re/im may be host or device memory, caller-owned, and
  * must outlive execution; host memory is read at every execute. */

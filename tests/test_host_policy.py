@@ -117,6 +117,39 @@ def test_spectral_registry():
     assert L.chirp_count() == 0
 
 
+def test_device_spectral_registry():
+    """chirp_register_spectral_device: valid ops register (a name replaces an
+    earlier host registration in place), invalid ones fail with a message;
+    the host application of a device op is its definition on host bins."""
+    import numpy as np
+    L = F.lib()
+    C = F.C
+    L.chirp_cleanup()
+    cb = C.SPECTRAL_FN(lambda re, im, n, ctx: None)
+    assert L.chirp_register_spectral(b"shape", cb, None) == 0
+    assert L.chirp_register_spectral_device(b"shape", C.CHIRP_DEVICE_GAIN, 0.5) == 0
+    assert L.chirp_register_spectral_device(b"late", C.CHIRP_DEVICE_DELAY, 3.25) == 1
+    assert L.chirp_count() == 2
+    assert L.chirp_register_spectral_device(b"bad", 9, 1.0) == -1
+    assert "unknown op" in C.error()
+    assert L.chirp_register_spectral_device(b"bad", C.CHIRP_DEVICE_LOWPASS, -1.0) == -1
+    assert L.chirp_register_spectral_device(b"", C.CHIRP_DEVICE_GAIN, 1.0) == -1
+    # host application: gain 0.5, then a 3.25-sample circular delay (n = 16)
+    nb, n = 9, 16
+    rng = np.random.default_rng(5)
+    re = rng.standard_normal(nb).astype(np.float32)
+    im = rng.standard_normal(nb).astype(np.float32)
+    t = C.faf_transform()
+    t.n = n
+    r2, i2 = re.copy(), im.copy()
+    for idx in (0, 1):
+        L.chirp_apply_split_f32(ctypes.byref(t), idx, 0, 0, r2.ctypes.data, i2.ctypes.data, nb)
+    k = np.arange(nb)
+    want = 0.5 * (re + 1j * im) * np.exp(-2j * np.pi * ((k * 3.25) % n) / n)
+    assert np.allclose(r2 + 1j * i2, want, atol=1e-6)
+    L.chirp_cleanup()
+
+
 def test_host_helpers():
     import numpy as np
     L = F.lib()
