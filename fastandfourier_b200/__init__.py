@@ -15,14 +15,14 @@ import ctypes
 
 from . import _lib as C
 from ._lib import (B_CUDA, DIR_FORWARD, DIR_INVERSE, FLAG_BLUESTEIN, FLAG_MEASURE,
-                   FLAG_TENSOR_CORE,
+                   FLAG_TENSOR_CORE, PREC_FP32, PREC_FP64,
                    L_DEFAULT, L_HERMITIAN, L_INTERLEAVED, L_REAL, L_SPLIT, N_DEFAULT,
                    N_FORWARD, N_NONE, N_ORTHO, T_FFT, T_IFFT, T_IRFFT, T_PIPELINE, T_RFFT,
                    T_STFT)
 
 __all__ = ["FafError", "Transform", "Uneven", "Server", "Request", "config", "lib", "available",
            "B_CUDA", "DIR_FORWARD", "DIR_INVERSE", "FLAG_TENSOR_CORE", "FLAG_BLUESTEIN",
-           "FLAG_MEASURE", "L_DEFAULT", "L_HERMITIAN",
+           "FLAG_MEASURE", "PREC_FP32", "PREC_FP64", "L_DEFAULT", "L_HERMITIAN",
            "L_INTERLEAVED", "L_REAL", "L_SPLIT", "N_DEFAULT", "N_FORWARD", "N_NONE", "N_ORTHO",
            "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
 
@@ -41,10 +41,10 @@ def available():
 
 
 def config(n, *, dir=DIR_FORWARD, norm=N_DEFAULT, layout=L_DEFAULT, flags=0, hop=0, win=0,
-           backend=0):
+           backend=0, precision=None):
     c = C.faf_config()
     c.n = n
-    c.precision = C.PREC_FP32
+    c.precision = C.PREC_FP32 if precision is None else precision
     c.dir = dir
     c.norm = norm
     c.layout = layout
@@ -86,11 +86,13 @@ def _check(rc):
 
 
 def _empty_like_batch(ref, shape):
+    """Output of `shape` beside `ref`: same device (torch) or host (numpy),
+    same floating type (float32, or float64 for FP64 transforms)."""
     if hasattr(ref, "data_ptr"):
         import torch
-        return torch.empty(shape, dtype=torch.float32, device=ref.device)
+        return torch.empty(shape, dtype=ref.dtype, device=ref.device)
     import numpy as np
-    return np.empty(shape, np.float32)
+    return np.empty(shape, ref.dtype)
 
 
 class Request:
@@ -234,14 +236,15 @@ class Transform:
 
     # ---- constructors (reference names) ----
     @classmethod
-    def fft(cls, n, *, inverse=False, norm=N_DEFAULT, layout=L_DEFAULT, flags=0):
+    def fft(cls, n, *, inverse=False, norm=N_DEFAULT, layout=L_DEFAULT, flags=0, precision=None):
         c = config(n, dir=DIR_INVERSE if inverse else DIR_FORWARD, norm=norm, layout=layout,
-                   flags=flags)
+                   flags=flags, precision=precision)
         return cls(C.lib().faf_create_fft(ctypes.byref(c)))
 
     @classmethod
-    def rfft(cls, n, *, inverse=False, norm=N_DEFAULT, layout=L_DEFAULT):
-        c = config(n, dir=DIR_INVERSE if inverse else DIR_FORWARD, norm=norm, layout=layout)
+    def rfft(cls, n, *, inverse=False, norm=N_DEFAULT, layout=L_DEFAULT, precision=None):
+        c = config(n, dir=DIR_INVERSE if inverse else DIR_FORWARD, norm=norm, layout=layout,
+                   precision=precision)
         return cls(C.lib().faf_create_rfft(ctypes.byref(c)))
 
     @classmethod

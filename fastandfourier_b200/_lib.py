@@ -15,7 +15,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfaf_b200.so")
 
 # enum values (include/fastandfourier.h)
-PREC_FP32, PREC_FP64 = 3, 4
+PREC_FP16, PREC_FP32, PREC_FP64 = 1, 3, 4
 (T_FFT, T_IFFT, T_RFFT, T_IRFFT) = (0, 1, 2, 3)
 T_STFT, T_PIPELINE = 12, 20
 L_DEFAULT, L_SPLIT, L_HERMITIAN, L_REAL, L_INTERLEAVED = 0, 1, 2, 3, 4

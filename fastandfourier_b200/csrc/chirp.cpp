@@ -322,6 +322,12 @@ faf_transform* compile_pipeline(const Node* p) {
     }
     faf_transform* fwd = compile_rfft(head, false);
     if (!fwd) return nullptr;
+    if (fwd->cfg.precision != FAF_PREC_FP32) {
+        fail("Chirp: the fused pipeline runs in FP32 on the CUDA backend (:precision f64 is "
+             "available for standalone (fft) / (rfft) forms)");
+        faf_destroy_transform(fwd);
+        return nullptr;
+    }
     faf_transform* inv = nullptr;
     if (has_inv) {
         if (tail->head == "inverse") {

@@ -275,15 +275,23 @@ float norm_scale(faf_norm norm, bool inverse, size_t n) {
     }
 }
 
-bool backend_ok(const faf_config& c) {
+double norm_scale64(faf_norm norm, bool inverse, size_t n) {
+    switch (norm) {
+    case FAF_NORM_ORTHO: return 1.0 / std::sqrt((double)n);
+    case FAF_NORM_FORWARD: return inverse ? 1.0 : 1.0 / (double)n;
+    default: return inverse ? 1.0 / (double)n : 1.0;
+    }
+}
+
+bool backend_ok(const faf_config& c, bool fp64_ok) {
     if (c.backend == FAF_BACKEND_VM || c.backend == FAF_BACKEND_JIT) {
         fail("backend %s is the reference's CPU engine; this library runs FAF_BACKEND_CUDA",
              c.backend == FAF_BACKEND_VM ? "VM" : "JIT");
         return false;
     }
-    if (c.precision != FAF_PREC_FP32) {
-        fail("the CUDA backend computes in FP32; precision '%s' is not available",
-             faf_precision_name(c.precision));
+    if (c.precision != FAF_PREC_FP32 && !(fp64_ok && c.precision == FAF_PREC_FP64)) {
+        fail("precision '%s' is not available for this transform on the CUDA backend (FP32; "
+             "FP64 for C2C, R2C and C2R)", faf_precision_name(c.precision));
         return false;
     }
     return true;
@@ -335,7 +343,12 @@ extern "C" faf_transform* faf_create_fft(const faf_config* cfg) {
         fail("FFT does not support norm '%s'", faf_norm_name(c.norm));
         return nullptr;
     }
-    if (!backend_ok(c)) return nullptr;
+    if (!backend_ok(c, true)) return nullptr;
+    const bool fp64 = c.precision == FAF_PREC_FP64;
+    if (fp64 && bluestein) {
+        fail("FP64 Bluestein transforms are not available on the CUDA backend");
+        return nullptr;
+    }
     if (c.n > (size_t)fafp::kMaxLength) {
         fail("FFT length %zu exceeds the 2^16 transform-length cap", c.n);
         return nullptr;
@@ -351,8 +364,10 @@ extern "C" faf_transform* faf_create_fft(const faf_config* cfg) {
         t->cfg.flags |= FAF_FLAG_BLUESTEIN;
     }
     std::string err;
-    DevicePlan* p = fafp::plan_c2c((int)c.n, inverse, norm_scale(c.norm, inverse, c.n),
-                                   t->flags, err);
+    DevicePlan* p = fp64 ? fafp::plan_c2c64((int)c.n, inverse, norm_scale64(c.norm, inverse, c.n),
+                                            err)
+                         : fafp::plan_c2c((int)c.n, inverse, norm_scale(c.norm, inverse, c.n),
+                                          t->flags, err);
     if (!p) {
         fail("CUDA plan for FFT n=%zu: %s", c.n, err.c_str());
         faf_destroy_transform(t);
@@ -397,7 +412,7 @@ extern "C" faf_transform* faf_create_rfft(const faf_config* cfg) {
         fail("R2C does not support norm '%s'", faf_norm_name(c.norm));
         return nullptr;
     }
-    if (!backend_ok(c)) return nullptr;
+    if (!backend_ok(c, true)) return nullptr;
     if (c.n > (size_t)fafp::kMaxLength) {
         fail("R2C length %zu exceeds the 2^16 transform-length cap", c.n);
         return nullptr;
@@ -415,13 +430,17 @@ extern "C" faf_transform* faf_create_rfft(const faf_config* cfg) {
     ic.norm = FAF_NORM_NONE;
     ic.dir = c.dir;
     ic.backend = c.backend;
+    ic.precision = c.precision;
     t->inner = faf_create_fft(&ic);
     if (!t->inner) {
         faf_destroy_transform(t);
         return nullptr;
     }
     std::string err;
-    DevicePlan* p = fafp::plan_r2c((int)c.n, inverse, norm_scale(c.norm, inverse, c.n), err);
+    DevicePlan* p =
+        c.precision == FAF_PREC_FP64
+            ? fafp::plan_r2c64((int)c.n, inverse, norm_scale64(c.norm, inverse, c.n), err)
+            : fafp::plan_r2c((int)c.n, inverse, norm_scale(c.norm, inverse, c.n), err);
     if (!p) {
         fail("CUDA plan for R2C n=%zu: %s", c.n, err.c_str());
         faf_destroy_transform(t);
@@ -439,6 +458,7 @@ extern "C" faf_transform* faf_create_stft(const faf_config* cfg) {
     faf_config c = *cfg;
     if (c.win_length == 0) c.win_length = c.n;
     if (c.hop_length == 0) c.hop_length = c.win_length / 4;
+    if (!backend_ok(c)) return nullptr;  // STFT runs in FP32
     if (c.win_length > c.n) {
         fail("STFT window length %zu exceeds FFT size %zu", c.win_length, c.n);
         return nullptr;

@@ -24,7 +24,8 @@ size_t next_5_smooth(size_t m);
 faf_transform* alloc_transform();
 void apply_resolved(faf_transform* t, const faf_config& c);
 float norm_scale(faf_norm norm, bool inverse, size_t n);
-bool backend_ok(const faf_config& c);
+double norm_scale64(faf_norm norm, bool inverse, size_t n);
+bool backend_ok(const faf_config& c, bool fp64_ok = false);
 
 int exec_split_one(const faf_transform* t, void* out_re, void* out_im, const void* in_re,
                    const void* in_im);

@@ -41,6 +41,7 @@ struct Request {
     long long batch = 1, in_dist = 0, out_dist = 0;
     bool interleaved = false;         // complex side interleaved
     bool framed = false;              // STFT: framed real signal
+    int scal = 1;                     // 4-byte words per scalar: 1 (FP32) or 2 (FP64)
     long long frames = 0, sig_len = 0;
 };
 
@@ -248,8 +249,9 @@ int run_host_chunked(const faf_transform* t, DevicePlan* p, Request& r, cudaStre
                      long long chunk) {
     if (ensure_copy_streams(p) != 0) return -1;
     const int nin = r.in_b ? 2 : 1, nout = r.out_b ? 2 : 1;
-    const size_t fin = span_floats(chunk, r.in_dist, r.in_len, r.in_fpe);
-    const size_t fout = span_floats(chunk, r.out_dist, r.out_len, r.out_fpe);
+    // sizes and offsets below count 4-byte words (two per FP64 value)
+    const size_t fin = span_floats(chunk, r.in_dist, r.in_len, r.in_fpe) * r.scal;
+    const size_t fout = span_floats(chunk, r.out_dist, r.out_len, r.out_fpe) * r.scal;
     // slot layout, each plane rounded to 64 floats (256 bytes)
     auto up = [](size_t f) { return (f + 63) & ~(size_t)63; };
     const size_t slot_floats = up(fin) * nin + up(fout) * nout;
@@ -271,10 +273,12 @@ int run_host_chunked(const faf_transform* t, DevicePlan* p, Request& r, cudaStre
         d.in_b = r.in_b ? slot + up(fin) : nullptr;
         d.out_a = slot + up(fin) * nin;
         d.out_b = r.out_b ? d.out_a + up(fout) : nullptr;
-        const size_t ioff = (size_t)b0 * r.in_dist * r.in_fpe;
-        const size_t ooff = (size_t)b0 * r.out_dist * r.out_fpe;
-        const size_t cin = span_floats(cb, r.in_dist, r.in_len, r.in_fpe) * sizeof(float);
-        const size_t cout = span_floats(cb, r.out_dist, r.out_len, r.out_fpe) * sizeof(float);
+        const size_t ioff = (size_t)b0 * r.in_dist * r.in_fpe * r.scal;
+        const size_t ooff = (size_t)b0 * r.out_dist * r.out_fpe * r.scal;
+        const size_t cin =
+            span_floats(cb, r.in_dist, r.in_len, r.in_fpe) * r.scal * sizeof(float);
+        const size_t cout =
+            span_floats(cb, r.out_dist, r.out_len, r.out_fpe) * r.scal * sizeof(float);
         // input copy: the slot's previous kernel has read its inputs
         if (i >= kSlots) e = cudaStreamWaitEvent(p->cp_h2d, p->ev_kern[s], 0);
         if (e == cudaSuccess)
@@ -336,8 +340,9 @@ int execute_request(const faf_transform* t, Request& r) {
     } else if (ndev == 0) {
         // Host buffers: copy in, run, copy out, synchronise.
         std::lock_guard<std::mutex> lock(p->mu);
-        const size_t fin = span_floats(r.batch, r.in_dist, r.in_len, r.in_fpe);
-        const size_t fout = span_floats(r.batch, r.out_dist, r.out_len, r.out_fpe);
+        // 4-byte words (two per FP64 value)
+        const size_t fin = span_floats(r.batch, r.in_dist, r.in_len, r.in_fpe) * r.scal;
+        const size_t fout = span_floats(r.batch, r.out_dist, r.out_len, r.out_fpe) * r.scal;
         const int nin = r.in_b ? 2 : 1, nout = r.out_b ? 2 : 1;
         const size_t total = (fin * nin + fout * nout) * sizeof(float) + 256;
         const size_t per_dir = std::max(fin * nin, fout * nout) * sizeof(float);
@@ -434,6 +439,31 @@ int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t s
     const long long in_dist = r.in_dist ? r.in_dist : (long long)r.in_len;
     const long long out_dist = r.out_dist ? r.out_dist : (long long)r.out_len;
     int launches = 1;
+    if (p->fp64) {
+        switch (t->type) {
+        case FAF_TRANSFORM_FFT:
+        case FAF_TRANSFORM_IFFT:
+            e = fafp::exec_c2c64(p, (const double*)r.in_a, (const double*)r.in_b,
+                                 (double*)r.out_a, (double*)r.out_b, r.batch, in_dist, out_dist,
+                                 r.interleaved, st);
+            break;
+        case FAF_TRANSFORM_RFFT:
+            if (r.interleaved) return fail("FP64 R2C output must be HERMITIAN split planes");
+            e = fafp::exec_r2c64(p, (const double*)r.in_a, (double*)r.out_a, (double*)r.out_b,
+                                 r.batch, in_dist, out_dist, st);
+            break;
+        case FAF_TRANSFORM_IRFFT:
+            if (r.interleaved) return fail("FP64 C2R input must be HERMITIAN split planes");
+            e = fafp::exec_c2r64(p, (const double*)r.in_a, (const double*)r.in_b,
+                                 (double*)r.out_a, r.batch, in_dist, out_dist, st);
+            break;
+        default:
+            return fail("FP64 is available for C2C, R2C and C2R transforms");
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "kernel launch");
+        note_launches(1);
+        return 0;
+    }
     switch (t->type) {
     case FAF_TRANSFORM_FFT:
     case FAF_TRANSFORM_IFFT:
@@ -489,7 +519,16 @@ int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t s
     return 0;
 }
 
+int build_request_typed(const faf_transform* t, faf_buffer* out, const faf_buffer* in,
+                        Request& r);
+
 int build_request(const faf_transform* t, faf_buffer* out, const faf_buffer* in, Request& r) {
+    r.scal = t->cfg.precision == FAF_PREC_FP64 ? 2 : 1;
+    return build_request_typed(t, out, in, r);
+}
+
+int build_request_typed(const faf_transform* t, faf_buffer* out, const faf_buffer* in,
+                        Request& r) {
     switch (t->type) {
     case FAF_TRANSFORM_PIPELINE: return check_pipeline(t, out, in, r);
     case FAF_TRANSFORM_RFFT:

@@ -150,6 +150,29 @@ int large_pot2_launches(int n1, int n2, long long batch);
 cudaError_t large_pot2_prepare(int n1, int n2);  // kernel attributes, before any capture
 cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st);
 
+// FP64 transforms (k_fp64.cu): kind 0 = C2C (C2C64Args), 1 = R2C, 2 = C2R
+// (Real64Args), on the FP64 runtime-radix engine, at most 512 threads per CTA.
+struct C2C64Args {
+    const double* in_re;
+    const double* in_im;   // NULL for interleaved
+    double* out_re;
+    double* out_im;        // NULL for interleaved
+    long long in_dist, out_dist, batch;
+    double scale, sgn;
+    int interleaved;
+};
+struct Real64Args {
+    const double* in_a;    // R2C: x; C2R: X re
+    const double* in_b;    // C2R: X im
+    double* out_a;         // R2C: X re; C2R: y
+    double* out_b;         // R2C: X im
+    long long in_dist, out_dist, batch;
+    double scale;
+    const double2* stw;    // super-twiddles, FP64
+};
+cudaError_t launch_fp64(int kind, const fafd::Shape& S, const Geometry& g, const double2* tw,
+                        const void* args, cudaStream_t st);
+
 // Overlap-add of the inverse STFT (k_istft.cu).
 cudaError_t launch_ola(const float* tmp, const float* w, int n, int win, int hop, long long F,
                        long long L, float* y, long long n_sig, cudaStream_t st);

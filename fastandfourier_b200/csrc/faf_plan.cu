@@ -308,6 +308,8 @@ void plan_free(DevicePlan* p) {
     cudaFree(p->d_rin);
     cudaFree(p->d_rout);
     cudaFree(p->d_window);
+    cudaFree(p->d_tw64);
+    cudaFree(p->d_stw64);
     cudaFree(p->d_tcB);
     cudaFree(p->d_tc_err);
     cudaFree(p->d_stage);
@@ -854,6 +856,116 @@ cudaError_t exec_istft(DevicePlan* p, const float* Xr, const float* Xi, float* y
     if (e != cudaSuccess) return e;
     return fafk::launch_ola(tmp, p->d_window, p->n, p->win, p->hop, frames, sig_len, y, n_sig,
                             st);
+}
+
+// ---- FP64 plans --------------------------------------------------------------
+
+static constexpr int kThreads64 = 512;
+
+static bool fp64_inner(DevicePlan* p, int m, std::string& err) {
+    if (!is_7_smooth(m)) {
+        err = "FP64 transforms need a 7-smooth (inner) length, got " + std::to_string(m);
+        return false;
+    }
+    if (!build_size(m, p->inner, err)) return false;
+    if (p->inner.T > kThreads64) {
+        err = "FP64 transforms of inner length " + std::to_string(m) +
+              " need more than one 512-thread CTA";
+        return false;
+    }
+    std::vector<double2> w((size_t)std::max(m, 1));
+    for (int i = 0; i < m; i++) {
+        const double a = -2.0 * M_PI * (double)i / (double)m;
+        w[i] = make_double2(std::cos(a), std::sin(a));
+    }
+    if (!cuda_ok(upload(&p->d_tw64, w.data(), w.size()), err, "FP64 twiddle upload")) return false;
+    p->fp64 = true;
+    return true;
+}
+
+DevicePlan* plan_c2c64(int n, bool inverse, double scale, std::string& err) {
+    DevicePlan* p = new_plan(Kind::C2C, n);
+    if (!fp64_inner(p, n, err)) {
+        plan_free(p);
+        return nullptr;
+    }
+    p->inverse = inverse;
+    p->scale64 = scale;
+    p->scale = (float)scale;
+    return p;
+}
+
+DevicePlan* plan_r2c64(int n, bool inverse, double scale, std::string& err) {
+    const int nc = n / 2;
+    DevicePlan* p = new_plan(inverse ? Kind::C2R : Kind::R2C, n);
+    if (!fp64_inner(p, nc, err)) {
+        plan_free(p);
+        return nullptr;
+    }
+    std::vector<double2> stw((size_t)std::max(1, nc / 2));
+    for (int k = 0; k < nc / 2; k++) {
+        const double ph = -M_PI * (((double)(k + 1) / (double)nc) + 0.5);
+        stw[k] = make_double2(std::cos(ph), std::sin(ph));
+    }
+    if (!cuda_ok(upload(&p->d_stw64, stw.data(), stw.size()), err, "FP64 super-twiddle upload")) {
+        plan_free(p);
+        return nullptr;
+    }
+    p->inverse = inverse;
+    p->scale64 = scale;
+    p->scale = (float)scale;
+    return p;
+}
+
+static fafk::Geometry geometry64(const FftSize& s, int slots, long long batch) {
+    fafk::Geometry g;
+    g.E = 16;
+    const size_t per = (size_t)2 * plane_floats(slots) * sizeof(double);
+    int G = std::max(1, kThreads64 / s.T);
+    G = (int)std::min<long long>(G, std::max(1LL, batch));
+    while (G > 1 && (size_t)G * per > kMaxSmem) G--;
+    g.G = G;
+    g.threads = G * s.T;
+    g.smem = (size_t)G * per;
+    g.staged = false;
+    return g;
+}
+
+cudaError_t exec_c2c64(DevicePlan* p, const double* in_re, const double* in_im, double* out_re,
+                       double* out_im, long long batch, long long in_dist, long long out_dist,
+                       bool interleaved, cudaStream_t st) {
+    fafk::C2C64Args a;
+    std::memset(&a, 0, sizeof a);
+    a.in_re = in_re; a.in_im = in_im; a.out_re = out_re; a.out_im = out_im;
+    a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
+    a.scale = p->scale64; a.sgn = p->inverse ? -1.0 : 1.0; a.interleaved = interleaved ? 1 : 0;
+    const int slots = p->inner.n;
+    return fafk::launch_fp64(0, p->inner.shape(slots), geometry64(p->inner, slots, batch),
+                             p->d_tw64, &a, st);
+}
+
+cudaError_t exec_r2c64(DevicePlan* p, const double* x, double* Xr, double* Xi, long long batch,
+                       long long in_dist, long long out_dist, cudaStream_t st) {
+    fafk::Real64Args a;
+    std::memset(&a, 0, sizeof a);
+    a.in_a = x; a.out_a = Xr; a.out_b = Xi;
+    a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
+    a.scale = p->scale64; a.stw = p->d_stw64;
+    const int slots = p->inner.n + 1;
+    return fafk::launch_fp64(1, p->inner.shape(slots), geometry64(p->inner, slots, batch),
+                             p->d_tw64, &a, st);
+}
+
+cudaError_t exec_c2r64(DevicePlan* p, const double* Xr, const double* Xi, double* y,
+                       long long batch, long long in_dist, long long out_dist, cudaStream_t st) {
+    fafk::Real64Args a;
+    std::memset(&a, 0, sizeof a);
+    a.in_a = Xr; a.in_b = Xi; a.out_a = y;
+    a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
+    a.scale = p->scale64; a.stw = p->d_stw64;
+    const int slots = p->inner.n + 1;
+    return fafk::launch_fp64(2, p->inner.shape(slots), geometry64(p->inner, slots, batch),
+                             p->d_tw64, &a, st);
 }
 
 }  // namespace fafp

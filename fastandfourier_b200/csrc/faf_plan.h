@@ -61,6 +61,7 @@ struct DevicePlan {
     int n = 0;             // outer length (real length for R2C family)
     bool inverse = false;  // C2C direction (conjugation trick)
     float scale = 1.0f;    // norm scale of this transform
+    double scale64 = 1.0;  // the same, FP64 plans
     float scale2 = 1.0f;   // pipeline: inverse-side scale
     FftSize inner;         // the FFT the kernels run
     // four-step path (inner complex length > kMaxSingleCta): n_inner = n1 * n2
@@ -77,6 +78,10 @@ struct DevicePlan {
     int* d_rin = nullptr;        // Rader gather
     int* d_rout = nullptr;       // Rader scatter
     float* d_window = nullptr;   // STFT window
+    // FP64 plans (FAF_PREC_FP64): FP64 twiddle tables of the inner size
+    bool fp64 = false;
+    double2* d_tw64 = nullptr;   // W_n^i, i < inner n
+    double2* d_stw64 = nullptr;  // R2C super-twiddles
     // tensor-core form (C2C, power of two): B = 16-point DFT as a 32 x 32
     // real FP16 matrix, hi then lo, in the MMA's shared-memory layout
     bool tc = false;
@@ -105,6 +110,17 @@ DevicePlan* plan_r2c(int n, bool inverse, float scale, std::string& err);
 DevicePlan* plan_pipeline(int n, float scale_fwd, float scale_inv, std::string& err);
 DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err);
 DevicePlan* plan_istft(int n, int win, int hop, std::string& err);
+// FP64 plans: single-CTA C2C of 5-smooth / codelet / 7-smooth lengths, and
+// R2C / C2R of even lengths whose half is such a length (up to 512 threads).
+DevicePlan* plan_c2c64(int n, bool inverse, double scale, std::string& err);
+DevicePlan* plan_r2c64(int n, bool inverse, double scale, std::string& err);
+cudaError_t exec_c2c64(DevicePlan* p, const double* in_re, const double* in_im, double* out_re,
+                       double* out_im, long long batch, long long in_dist, long long out_dist,
+                       bool interleaved, cudaStream_t st);
+cudaError_t exec_r2c64(DevicePlan* p, const double* x, double* Xr, double* Xi, long long batch,
+                       long long in_dist, long long out_dist, cudaStream_t st);
+cudaError_t exec_c2r64(DevicePlan* p, const double* Xr, const double* Xi, double* y,
+                       long long batch, long long in_dist, long long out_dist, cudaStream_t st);
 void plan_free(DevicePlan* p);
 
 // Device-pointer executes (enqueue on `st`).

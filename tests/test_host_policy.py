@@ -57,12 +57,16 @@ def test_cpu_backends_are_refused():
         assert name in F.C.error() and "FAF_BACKEND_CUDA" in F.C.error()
 
 
-def test_fp64_is_refused_on_the_cuda_backend():
+def test_fp64_only_where_available():
+    """FP64 runs C2C, R2C and C2R; STFT (and the fused pipeline) stay FP32
+    and refuse FP64 at create with a message."""
     L = F.lib()
-    c = F.config(64)
-    c.precision = F.C.PREC_FP64
+    c = F.config(1024, hop=256, win=1024, precision=F.C.PREC_FP64)
+    assert not L.faf_create_stft(ctypes.byref(c))
+    assert "FP32" in F.C.error() and "FP64" in F.C.error()
+    c = F.config(64, precision=F.C.PREC_FP16)
     assert not L.faf_create_fft(ctypes.byref(c))
-    assert "FP32" in F.C.error()
+    assert "not available" in F.C.error()
 
 
 def test_length_cap():
