@@ -184,11 +184,16 @@ struct NoHook {
     __device__ __forceinline__ void operator()() const {}
 };
 
-template <int N, int S, bool TWS_SMEM, class Src, class Snk, class Sync, class Hook>
+// Stages S.. of the transform.  SKIP_LAST stops before the last stage (the
+// caller runs it, fused with what follows; the stage before it has written
+// the workspace and synchronised).
+template <int N, int S, bool TWS_SMEM, class Src, class Snk, class Sync, class Hook,
+          bool SKIP_LAST = false>
 __device__ __forceinline__ void ct_run(float (&xr)[16], float (&xi)[16], int t, float2* ws,
                                        const float2* __restrict__ tws, const Src& src,
                                        const Snk& snk, const Sync& sync, const Hook& hook) {
     using Pl = P2<N>;
+    static_assert(!SKIP_LAST || Pl::NS >= 2, "a skipped last stage needs an earlier one");
     const SmemC mid{ws};
     const LastC<Snk> last{snk};
     if constexpr (Pl::NS == 1) {
@@ -205,12 +210,14 @@ __device__ __forceinline__ void ct_run(float (&xr)[16], float (&xi)[16], int t, 
         // stage 0 ends with a barrier: the source is no longer read by anyone
         ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid, sync);
         hook();
-        ct_run<N, 1, TWS_SMEM>(xr, xi, t, ws, tws, mid, snk, sync, NoHook());
+        ct_run<N, 1, TWS_SMEM, SmemC, Snk, Sync, NoHook, SKIP_LAST>(xr, xi, t, ws, tws, mid, snk,
+                                                                    sync, NoHook());
     } else if constexpr (S == Pl::NS - 1) {
-        ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, last, sync);
+        if constexpr (!SKIP_LAST) ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, last, sync);
     } else {
         ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, mid, sync);
-        ct_run<N, S + 1, TWS_SMEM>(xr, xi, t, ws, tws, mid, snk, sync, NoHook());
+        ct_run<N, S + 1, TWS_SMEM, SmemC, Snk, Sync, NoHook, SKIP_LAST>(xr, xi, t, ws, tws, mid,
+                                                                        snk, sync, NoHook());
     }
 }
 
@@ -224,6 +231,82 @@ __device__ __forceinline__ void ct_fft(int t, float2* ws, const float2* __restri
     float xr[16], xi[16];
     if constexpr (!Src::kSmem) sync();
     ct_run<N, 0, TWS_SMEM>(xr, xi, t, ws, tws, src, snk, sync, hook);
+}
+
+// Every stage but the last, from a global source; the workspace holds the
+// last stage's input when it returns (synchronised).
+template <int N, bool TWS_SMEM, class Src, class Sync>
+__device__ __forceinline__ void ct_fft_but_last(int t, float2* ws, const float2* __restrict__ tws,
+                                                const Src& src, const Sync& sync) {
+    float xr[16], xi[16];
+    if constexpr (!Src::kSmem) sync();
+    ct_run<N, 0, TWS_SMEM, Src, SmemC, Sync, NoHook, true>(xr, xi, t, ws, tws, src, SmemC{ws},
+                                                           sync, NoHook());
+}
+
+// The last stage of an N-point transform whose last radix is 8 (two
+// butterflies per thread), run so that each thread holds both ends of its
+// Hermitian bin pairs (k, N - k) in registers.  The last stage's span equals
+// its butterfly count NB, so butterfly b writes Z[b + r NB], and the partner
+// of bin b1 + r NB is (NB - b1) + (R - 1 - r) NB: thread t takes butterflies
+// t and NB - t (thread 0: 0 and NB / 2, each paired with itself).  Calls
+// dc(Z[0]) once, and pair(k, Z[k], Z[N - k]) once for every 1 <= k <= N / 2
+// (k = N / 2 paired with itself); all bins it touches are the thread's own.
+template <int N>
+struct LastPairs {
+    using Pl = P2<N>;
+    static constexpr int S = Pl::NS - 1;
+    static constexpr int R = Pl::radix(S);
+    static constexpr bool ok = Pl::NS >= 2 && R == 8;
+};
+
+template <int N, bool TWS_SMEM, class Dc, class Pair>
+__device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
+                                              const float2* __restrict__ tws, const Dc& dc,
+                                              const Pair& pair) {
+    using Pl = P2<N>;
+    constexpr int S = Pl::NS - 1, R = Pl::radix(S), P = Pl::span(S), NB = N / R;
+    constexpr int OFF = Pl::tw_offset(S);
+    static_assert(LastPairs<N>::ok && P == NB && Pl::T == NB / 2, "radix-8 last stage");
+    const int b[2] = {t, t == 0 ? NB / 2 : NB - t};
+    float xr[2][R], xi[2][R];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const float2* p = ws + pad2(b[h]);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const float2 v = p[r * (NB + NB / 16)];
+            xr[h][r] = v.x;
+            xi[h][r] = v.y;
+        }
+        if (b[h] != 0) {
+            const float2* w = tws + OFF + b[h];
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                const float2 wr = TWS_SMEM ? w[(r - 1) * P] : __ldg(&w[(r - 1) * P]);
+                cmul_inplace(xr[h][r], xi[h][r], wr.x, wr.y);
+            }
+        }
+        Dft<R>::run(xr[h], xi[h]);
+    }
+    auto Z = [&](int h, int r) {
+        const int j = Dft<R>::slot(r);
+        return cf{xr[h][j], xi[h][j]};
+    };
+    if (t != 0) {
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int k1 = b[0] + r * NB, k2 = N - k1;
+            if (k1 < k2) pair(k1, Z(0, r), Z(1, R - 1 - r));
+            else pair(k2, Z(1, R - 1 - r), Z(0, r));
+        }
+    } else {
+        dc(Z(0, 0));
+#pragma unroll
+        for (int r = 1; r <= R / 2; r++) pair(r * NB, Z(0, r), Z(0, R - r));
+#pragma unroll
+        for (int r = 0; r < R / 2; r++) pair(NB / 2 + r * NB, Z(1, r), Z(1, R - 1 - r));
+    }
 }
 
 // ---- asynchronous input staging (cp.async, 16-byte chunks) ---------------

@@ -103,6 +103,31 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
             fafct::cp_async_wait_all();
             ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{q.stage}, mid, q.sync,
                               PrefetchNext<N>{q.stage, xn, q.t});
+        } else if constexpr (fafct::LastPairs<N>::ok) {
+            // last stage fused with the post-pass: no workspace round trip
+            fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw,
+                                              RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
+                                              q.sync);
+            if (live) {
+                const long long oo = bi * a.out_dist * fpe;
+                const HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo,
+                                   a.interleaved};
+                const float sc = a.scale;
+                const float2* __restrict__ stw = a.stw;
+                fafct::ct_last_pairs<N, kTw<N>>(
+                    q.t, q.ws, q.tw,
+                    [&](cf z) {
+                        out.put(0, (z.x + z.y) * sc, 0.f);
+                        out.put(N, (z.x - z.y) * sc, 0.f);
+                    },
+                    [&](int k, cf zk, cf zn) {
+                        cf Xk, Xnk;
+                        r2c_pair(zk, zn, __ldg(&stw[k - 1]), Xk, Xnk);
+                        if (k != N - k) out.put(k, Xk.x * sc, Xk.y * sc);
+                        out.put(N - k, Xnk.x * sc, Xnk.y * sc);
+                    });
+            }
+            continue;
         } else {
             ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
                               mid, q.sync);
@@ -211,11 +236,38 @@ __device__ __forceinline__ void pipe_middle(int t, const SmemC& mid,
     }
 }
 
+// The same bin-pair pass fused with the forward transform's last stage
+// (fafct::ct_last_pairs): each thread transforms the bins it owns in
+// registers and writes the pre-pass result back to those same slots.
+template <int N, class Ops>
+__device__ __forceinline__ void pipe_middle_fused(int t, float2* ws, const float2* tw,
+                                                  const float2* __restrict__ stw, const Ops& ops) {
+    const SmemC mid{ws};
+    fafct::ct_last_pairs<N, kTw<N>>(
+        t, ws, tw,
+        [&](cf z) {
+            const cf x0 = ops(0, cf{z.x + z.y, 0.f});
+            const cf xn = ops(N, cf{z.x - z.y, 0.f});
+            mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
+        },
+        [&](int k, cf zk, cf zn) {
+            const float2 w = __ldg(&stw[k - 1]);
+            cf Xk, Xnk;
+            r2c_pair(zk, zn, w, Xk, Xnk);
+            if (k == N - k) Xk = Xnk;
+            Xk = ops(k, Xk);
+            Xnk = (k == N - k) ? Xk : ops(N - k, Xnk);
+            cf Zk, Znk;
+            c2r_pair(Xk, Xnk, w, Zk, Znk);
+            if (k != N - k) mid.put(k, Zk);
+            mid.put(N - k, Znk);
+        });
+}
+
 template <int N, bool ASYNC>
 __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ tws,
                                                     const RealArgs a, int G, bool vec) {
     extern __shared__ float4 smem4[];
-    constexpr int nc = N, T = P2<N>::T;
     CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws, ASYNC);
     const SmemC mid{q.ws};
     if constexpr (ASYNC) {
@@ -232,15 +284,25 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
             fafct::cp_async_wait_all();
             ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{q.stage}, mid, q.sync,
                               PrefetchNext<N>{q.stage, xn, q.t});
+        } else if constexpr (fafct::LastPairs<N>::ok) {
+            fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw,
+                                              RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
+                                              q.sync);
+            if (ops_single_mul(a))
+                pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsMul1{&a.ops[0]});
+            else
+                pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsAny{&a});
         } else {
             ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
                               mid, q.sync);
         }
-        q.sync();
-        if (ops_single_mul(a))
-            pipe_middle<N>(q.t, mid, a.stw, OpsMul1{&a.ops[0]});
-        else
-            pipe_middle<N>(q.t, mid, a.stw, OpsAny{&a});
+        if constexpr (!fafct::LastPairs<N>::ok || ASYNC) {
+            q.sync();
+            if (ops_single_mul(a))
+                pipe_middle<N>(q.t, mid, a.stw, OpsMul1{&a.ops[0]});
+            else
+                pipe_middle<N>(q.t, mid, a.stw, OpsAny{&a});
+        }
         q.sync();
         ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
                           RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec}, q.sync);
