@@ -10,7 +10,8 @@ once, each output sample written once: 8 bytes per sample) and its fraction
 of the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload pipeline|r2c|c2c1024|c2c16384|c2c16384tc|stft|uneven|serve]
+                    [--workload pipeline|r2c|c2c1024|c2c16384|c2c16384tc|c2c4096fp64|
+                                stft|istft|uneven|serve]
 
 --workload serve replays a Poisson request trace (20k requests/s: 40% rfft
 of log-uniform sizes 256..65536 rounded to the recommended size, 30% the
@@ -78,6 +79,11 @@ WORKLOADS = {
                None, 4096, None, None),
 }
 
+WORKLOADS["c2c4096fp64"] = ("C2C n=4096 batch 4096 forward in FP64 (split planes, FAF_PREC_FP64), "
+                            "U[-1,1), seed 0", 4096, 4096, 32 * 4096, 5 * 4096 * 12)
+WORKLOADS["istft"] = ("inverse STFT Hann 1024 hop 256: 64 signals x 1021 frames x 513 bins -> "
+                      "2^18 samples, N(0,1) frames, seed 4", 1024, 64, None, None)
+
 WORKLOADS["serve"] = ("serving trace: 4000 requests, Poisson 20k req/s (seed 4); 40% rfft "
                       "N log-uniform [256, 65536] -> recommended size, 30% notch pipeline "
                       "4096, 30% STFT Hann 1024 hop 256 over L log-uniform [2^16, 2^20]; "
@@ -99,6 +105,14 @@ def make_inputs(workload, batch):
         x = rng.standard_normal((batch, n), dtype=np.float32)
         x += (5 * np.cos(2 * np.pi * 410 * k / n)).astype(np.float32)
         return [x]
+    if workload == "c2c4096fp64":
+        rng = np.random.default_rng(0)
+        return [rng.uniform(-1, 1, (batch, n)), rng.uniform(-1, 1, (batch, n))]
+    if workload == "istft":
+        rng = np.random.default_rng(4)
+        F_ = stft_geometry(1 << 18)[0]
+        return [rng.standard_normal((batch, F_, 513), dtype=np.float32),
+                rng.standard_normal((batch, F_, 513), dtype=np.float32)]
     if workload.startswith("c2c"):
         seed = 0 if workload == "c2c1024" else 3
         rng = np.random.default_rng(seed)
@@ -127,7 +141,7 @@ def stft_geometry(L, n=1024, win=1024, hop=256):
 def algorithmic_bytes(workload, batch):
     if workload == "uneven":
         return 16 * sum(uneven_lengths(batch))
-    if workload == "stft":
+    if workload in ("stft", "istft"):
         L = 1 << 18
         F, bins = stft_geometry(L)
         return batch * (4 * L + 8 * bins)
@@ -229,6 +243,10 @@ def build_transform(F, workload, torch):
         return F.Transform.rfft(n)
     if workload == "c2c16384tc":
         return F.Transform.fft(n, flags=F.FLAG_TENSOR_CORE)
+    if workload == "c2c4096fp64":
+        return F.Transform.fft(n, precision=F.PREC_FP64)
+    if workload == "istft":
+        return F.Transform.istft(1024, win=1024, hop=256)
     if workload.startswith("c2c"):
         return F.Transform.fft(n)
     if workload == "stft":
@@ -247,6 +265,8 @@ def run_step(F, t, workload, ins, outs, plain=False):
         t.c2c(ins[0], ins[1], out_re=outs[0], out_im=outs[1])
     elif workload == "stft":
         t.stft_frames(ins[0], out_re=outs[0], out_im=outs[1])
+    elif workload == "istft":
+        t.istft_frames(ins[0], ins[1], out=outs[0])
     elif workload == "uneven":
         if hasattr(ins[0], "data_ptr"):
             t.execute(ins[0], ins[1], outs[0], outs[1], plain=plain)
@@ -270,10 +290,11 @@ def run_step(F, t, workload, ins, outs, plain=False):
 def alloc_outputs(workload, batch, like, torch):
     n = WORKLOADS[workload][1]
     # torch tensors -> device outputs; numpy inputs -> pinned host numpy outputs
+    dt = torch.float64 if workload == "c2c4096fp64" else torch.float32
     if hasattr(like, "data_ptr"):
-        mk = lambda shp: torch.empty(shp, dtype=torch.float32, device=like.device)  # noqa: E731
+        mk = lambda shp: torch.empty(shp, dtype=dt, device=like.device)  # noqa: E731
     else:
-        mk = lambda shp: torch.empty(shp, dtype=torch.float32, pin_memory=True).numpy()  # noqa: E731
+        mk = lambda shp: torch.empty(shp, dtype=dt, pin_memory=True).numpy()  # noqa: E731
     if workload == "pipeline":
         return [mk((batch, n))]
     if workload == "r2c":
@@ -283,6 +304,8 @@ def alloc_outputs(workload, batch, like, torch):
     if workload == "stft":
         F_, bins = stft_geometry(1 << 18)
         return [mk((batch, F_, 513)), mk((batch, F_, 513))]
+    if workload == "istft":
+        return [mk((batch, 1 << 18))]
     if workload == "uneven":
         total = sum(uneven_lengths(batch))
         return [mk((total,)), mk((total,))]
@@ -435,7 +458,8 @@ def run_ours(args, rank, world, local_rank):
                 "traffic": ncu_traffic(workload),
                 "algorithmic_bytes_per_launch": nbytes,
                 "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
-                           "uneven": "k_uneven_large", "c2c16384tc": "k2_c2c_tc"}.get(
+                           "uneven": "k_uneven_large", "c2c16384tc": "k2_c2c_tc",
+                           "c2c4096fp64": "k64_c2c", "istft": "k2_c2r + k_ola"}.get(
                                workload, "k2_c2c")}
 
     cpu = None
@@ -454,7 +478,7 @@ def run_ours(args, rank, world, local_rank):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32",
+            "dtype": "f64" if workload == "c2c4096fp64" else "f32",
             "data": "synthetic (seeded numpy PCG64)",
             "config": {"workload": desc, "n": n, "batch_per_gpu": batch,
                        "parallelism": f"replicas{world}",
@@ -504,6 +528,13 @@ def _ref_call(refimpl, workload, sample_inputs, threads):
                          sample_inputs[0], m, z, threads=threads)
     elif workload == "r2c":
         refimpl.r2c(sample_inputs[0], threads=threads)
+    elif workload == "c2c4096fp64":
+        refimpl.c2c64(sample_inputs[0], sample_inputs[1], threads=threads)
+    elif workload == "istft":
+        # the reference has no inverse STFT: the oracle's restatement (FP64
+        # numpy, one core) stands in for it
+        from oracle import orc
+        orc.istft(sample_inputs[0], sample_inputs[1], 1024, 1024, 256)
     elif workload.startswith("c2c"):
         refimpl.c2c(sample_inputs[0], sample_inputs[1], threads=threads)
     elif workload == "stft":
@@ -554,6 +585,8 @@ def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
     want = WORKLOADS[workload][2]
     if workload == "stft":
         want = max(1, min(want, threads))
+    elif workload == "istft":
+        want = 2
     elif workload == "uneven":
         want = 512
     sample, nbytes, sample_b = cpu_sample(workload, host_in, want)
@@ -566,6 +599,11 @@ def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
         if el >= seconds or reps >= 1000:
             break
     gbs = reps * nbytes / el / 1e9
+    if workload == "istft":
+        return {"value": round(gbs, 3), "unit": "GB/s", "cores": 1, "kind": "port",
+                "sample": f"{reps} passes x {sample_b} signals of the workload ({el:.1f} s, "
+                          "the oracle's FP64 numpy restatement: the reference has no inverse "
+                          "STFT)"}
     return {"value": round(gbs, 3), "unit": "GB/s", "cores": threads, "kind": "reference",
             "isa": refimpl.isa(),
             "sample": f"{reps} passes x {sample_b} transforms of the workload "
@@ -590,6 +628,8 @@ def run_reference(args, rank, world):
     want = min(batch, max(threads * 8, 64)) if workload != "stft" else min(batch, threads)
     if workload == "uneven":
         want = min(batch, max(threads * 4, 64))
+    if workload == "istft":
+        want, threads = 2, 1  # the single-core oracle restatement
     sample, nbytes, sample_b = cpu_sample(workload, host_in, want)
     for _ in range(max(args.warmup, 1)):
         _ref_call(refimpl, workload, sample, threads)
@@ -616,7 +656,8 @@ def run_reference(args, rank, world):
         "data": "synthetic (seeded numpy PCG64)",
         "config": {"workload": desc, "n": n, "batch_per_gpu": batch, "parallelism": "host cores"},
         "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads,
-                         "kind": "reference", "isa": refimpl.isa(),
+                         "kind": "port" if workload == "istft" else "reference",
+                         "isa": refimpl.isa(),
                          "sample": f"{sample_b} of {batch} transforms per step, median of "
                                    f"{args.steps} steps"},
         "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,

@@ -51,6 +51,7 @@ typedef struct {
     size_t b0, b1;     /* batch slice [b0, b1) */
     const float *in_re, *in_im;
     float *out_re, *out_im;
+    int f64;           /* C2C: buffers hold doubles, transform in FAF_PREC_FP64 */
     int rc;
 } job;
 
@@ -62,6 +63,7 @@ static faf_transform *make_transform(const job *j) {
     case JOB_C2C:
         c.layout = FAF_LAYOUT_SPLIT;
         c.dir = j->inverse ? FAF_DIR_INVERSE : FAF_DIR_FORWARD;
+        if (j->f64) c.precision = FAF_PREC_FP64;
         return faf_create_fft(&c);
     case JOB_R2C:
     case JOB_STFT:
@@ -104,11 +106,13 @@ static void *run_job(void *arg) {
         faf_buffer in, out;
         int rc = 0;
         switch (j->kind) {
-        case JOB_C2C:
-            in = faf_buffer_split((void *)(j->in_re + b * n), (void *)(j->in_im + b * n), n);
-            out = faf_buffer_split(j->out_re + b * n, j->out_im + b * n, n);
+        case JOB_C2C: {
+            const size_t o = b * n * (j->f64 ? 2 : 1);  /* in floats */
+            in = faf_buffer_split((void *)(j->in_re + o), (void *)(j->in_im + o), n);
+            out = faf_buffer_split(j->out_re + o, j->out_im + o, n);
             rc = faf_execute(t, &out, &in);
             break;
+        }
         case JOB_R2C:
             in = faf_buffer_real((void *)(j->in_re + b * n), n);
             out = faf_buffer_hermitian(j->out_re + b * nb, j->out_im + b * nb, nb);
@@ -178,6 +182,17 @@ int refdrv_c2c(size_t n, int inverse, int norm, uint32_t flags, size_t batch,
     memset(&j, 0, sizeof(j));
     j.kind = JOB_C2C; j.n = n; j.inverse = inverse; j.norm = norm; j.flags = flags;
     j.in_re = in_re; j.in_im = in_im; j.out_re = out_re; j.out_im = out_im;
+    return run_batched(&j, batch, nthreads);
+}
+
+/* The same in FP64 (double buffers, FAF_PREC_FP64 transforms). */
+int refdrv_c2c64(size_t n, int inverse, int norm, size_t batch, const double *in_re,
+                 const double *in_im, double *out_re, double *out_im, int nthreads) {
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_C2C; j.n = n; j.inverse = inverse; j.norm = norm; j.f64 = 1;
+    j.in_re = (const float *)in_re; j.in_im = (const float *)in_im;
+    j.out_re = (float *)out_re; j.out_im = (float *)out_im;
     return run_batched(&j, batch, nthreads);
 }
 

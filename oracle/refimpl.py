@@ -68,6 +68,8 @@ def lib():
         L.refdrv_error.restype = ctypes.c_char_p
         L.refdrv_c2c.argtypes = [sz, i, i, u32, sz, _f32p, _f32p, _f32p, _f32p, i]
         L.refdrv_r2c.argtypes = [sz, i, sz, _f32p, _f32p, _f32p, i]
+        f64p = ctypes.POINTER(ctypes.c_double)
+        L.refdrv_c2c64.argtypes = [sz, i, i, sz, f64p, f64p, f64p, f64p, i]
         L.refdrv_c2r.argtypes = [sz, i, sz, _f32p, _f32p, _f32p, i]
         L.refdrv_pipeline.argtypes = [ctypes.c_char_p, sz, _f32p, _f32p, sz, sz,
                                       _f32p, _f32p, i]
@@ -100,6 +102,18 @@ def c2c(re, im, inverse=False, norm=1, flags=0, threads=1):
     yr, yi = np.empty_like(re), np.empty_like(im)
     _check(lib().refdrv_c2c(n, int(inverse), norm, flags, re.size // n,
                             _p(re), _p(im), _p(yr), _p(yi), threads))
+    return yr, yi
+
+
+def c2c64(re, im, inverse=False, norm=1, threads=1):
+    """The reference's FP64 C2C (FAF_PREC_FP64) on double split planes."""
+    re = np.ascontiguousarray(re, dtype=np.float64)
+    im = np.ascontiguousarray(im, dtype=np.float64)
+    n = re.shape[-1]
+    yr, yi = np.empty_like(re), np.empty_like(im)
+    p = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))  # noqa: E731
+    _check(lib().refdrv_c2c64(n, int(inverse), norm, re.size // n, p(re), p(im), p(yr), p(yi),
+                              threads))
     return yr, yi
 
 

@@ -33,6 +33,24 @@ def test_fp64_c2c(cuda, n, inverse):
     assert rel(hr + 1j * hi, want) <= TOL64
 
 
+@pytest.mark.parametrize("n", [60, 1024, 4096])
+def test_fp64_c2c_vs_reference(cuda, n):
+    """Against the reference's own FP64 C2C (src/faf_core.c:521, FAF_PREC_FP64),
+    compiled from its sources into the oracle's reference library."""
+    import fastandfourier_b200 as F
+    from oracle import refimpl
+    if not refimpl.available():
+        pytest.skip("reference library not built")
+    rng = seeded(980 + n)
+    re = rng.uniform(-1, 1, (6, n))
+    im = rng.uniform(-1, 1, (6, n))
+    for inverse in (False, True):
+        t = F.Transform.fft(n, inverse=inverse, precision=F.PREC_FP64)
+        gr, gi = t.c2c(re, im)
+        wr, wi = refimpl.c2c64(re, im, inverse=inverse)
+        assert rel(gr + 1j * gi, wr + 1j * wi) <= TOL64
+
+
 def test_fp64_c2c_interleaved(cuda):
     import fastandfourier_b200 as F
     rng = seeded(950)

@@ -151,3 +151,20 @@ def test_hann_matches_definition():
     i = np.arange(n)
     assert np.allclose(w, 0.5 * (1 - np.cos(2 * np.pi * i / (n - 1))), atol=1e-6)
     assert w[0] == 0 and abs(w[-1]) < 1e-6
+
+
+@pytest.mark.parametrize("n", [60, 1024, 4096])
+def test_reference_fp64_c2c_vs_numpy(n):
+    """The reference's FP64 C2C path (src/faf_core.c:521) as the driver calls
+    it agrees with numpy's FP64 FFT, so it can stand as the FP64 checker."""
+    from oracle import refimpl
+    if not refimpl.available():
+        pytest.skip("reference library not built")
+    rng = np.random.default_rng(n)
+    re, im = rng.uniform(-1, 1, (3, n)), rng.uniform(-1, 1, (3, n))
+    for inv in (False, True):
+        yr, yi = refimpl.c2c64(re, im, inverse=inv)
+        z = re + 1j * im
+        want = np.fft.ifft(z, axis=-1) if inv else np.fft.fft(z, axis=-1)
+        got = yr + 1j * yi
+        assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-12
