@@ -80,6 +80,22 @@ def _buf(re, im, n, layout):
     return b
 
 
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: the legacy default stream as an explicit handle
+
+
+def _stream_handle(stream):
+    """cudaStream_t for the C ABI.  None (or a raw 0) is NULL: the library's
+    default, synchronous execute.  A torch stream whose handle is 0 is torch's
+    default stream, the legacy stream; it is passed as cudaStreamLegacy so
+    that work is enqueued there without a host synchronisation."""
+    if stream is None:
+        return None
+    h = getattr(stream, "cuda_stream", None)
+    if h is None:
+        return int(stream) or None
+    return int(h) or CUDA_STREAM_LEGACY
+
+
 def _check(rc):
     if rc != 0:
         raise FafError(C.error())
@@ -205,8 +221,7 @@ class Uneven:
         return C.lib().faf_uneven_total(self._p)
 
     def set_stream(self, stream):
-        h = getattr(stream, "cuda_stream", stream)
-        _check(C.lib().faf_uneven_set_stream(self._p, h or None))
+        _check(C.lib().faf_uneven_set_stream(self._p, _stream_handle(stream)))
 
     def execute(self, re, im, out_re, out_im, plain=False):
         f = C.lib().faf_uneven_execute_plain if plain else C.lib().faf_uneven_execute
@@ -298,8 +313,7 @@ class Transform:
 
     def set_stream(self, stream):
         """stream: torch.cuda.Stream, a raw cudaStream_t int, or None."""
-        h = getattr(stream, "cuda_stream", stream)
-        _check(C.lib().faf_cuda_set_stream(self._p, h or None))
+        _check(C.lib().faf_cuda_set_stream(self._p, _stream_handle(stream)))
 
     def synchronize(self):
         _check(C.lib().faf_cuda_synchronize(self._p))

@@ -47,7 +47,8 @@ int faf_cuda_last_launches(void);
 
 /* Enqueue this transform's work on `stream` (a cudaStream_t).  With a stream
  * set, faf_execute on device buffers returns without synchronising.  NULL
- * restores the default (legacy stream, synchronous execute). */
+ * restores the default (legacy stream, synchronous execute); to enqueue on
+ * the legacy stream without synchronising, pass cudaStreamLegacy. */
 int faf_cuda_set_stream(faf_transform *t, void *stream);
 void *faf_cuda_get_stream(const faf_transform *t);
 int faf_cuda_synchronize(const faf_transform *t);

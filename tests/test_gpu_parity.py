@@ -299,6 +299,26 @@ def test_user_stream_async(cuda):
     assert orc.rel_l2_complex(host(yr), host(yi), orc.fp64_c2c(re, im)) <= REL_L2_TOL
 
 
+def test_default_torch_stream_is_asynchronous(cuda):
+    """torch's default stream (handle 0) is set as cudaStreamLegacy: execute
+    enqueues on it without synchronising, and stream order keeps results
+    right for a consumer on the same stream."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n = 4096
+    t = F.Transform.rfft(n)
+    t.set_stream(torch.cuda.current_stream())
+    assert F.lib().faf_cuda_get_stream(t._p) == F.CUDA_STREAM_LEGACY
+    x = seeded(16).standard_normal((256, n)).astype(np.float32)
+    xd = dev(torch, x)
+    Xr, Xi = t.r2c(xd)
+    got = (Xr * 2).cpu().numpy() + 1j * (Xi * 2).cpu().numpy()  # same-stream consumer
+    want = 2 * np.fft.rfft(x.astype(np.float64), axis=-1)
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= REL_L2_TOL
+    t.set_stream(None)
+    assert F.lib().faf_cuda_get_stream(t._p) is None
+
+
 def test_config1_c2c_forward_inverse(cuda):
     """C2C N=1024, batch 256, NumPy norm, forward then inverse, seed 0."""
     import fastandfourier_b200 as F

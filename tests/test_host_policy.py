@@ -201,3 +201,20 @@ def test_uneven_rejects_illegal_lengths():
         F.Uneven([60, 23])
     with pytest.raises(F.FafError, match="empty"):
         F.Uneven([])
+
+
+def test_stream_handles():
+    """None is the library's synchronous default; torch's default stream
+    (handle 0, the legacy stream) becomes cudaStreamLegacy so execution stays
+    asynchronous on it; other handles pass through."""
+    import fastandfourier_b200 as F
+
+    class S:  # stands in for torch.cuda.Stream
+        def __init__(self, h):
+            self.cuda_stream = h
+
+    assert F._stream_handle(None) is None
+    assert F._stream_handle(0) is None
+    assert F._stream_handle(S(0)) == F.CUDA_STREAM_LEGACY == 1
+    assert F._stream_handle(S(0x7f00deadbe00)) == 0x7f00deadbe00
+    assert F._stream_handle(0x5000) == 0x5000
