@@ -318,6 +318,14 @@ class Transform:
     def synchronize(self):
         _check(C.lib().faf_cuda_synchronize(self._p))
 
+    def wait_status(self):
+        """0: every bounded wait of this transform's kernels completed; 1: one
+        ran out (that launch's results are invalid)."""
+        rc = C.lib().faf_cuda_wait_status(self._p)
+        if rc < 0:
+            raise FafError(C.error())
+        return rc
+
     def tc_status(self):
         """Tensor-core plans: 0 = every MMA wait completed, 1 = one ran out of
         its bound; -1 for other plans."""

@@ -132,6 +132,7 @@ _SIGS = [
     ("faf_cuda_create_istft", TP, [ctypes.POINTER(faf_config)]),
     ("faf_cuda_set_stream", ctypes.c_int, [TP, ctypes.c_void_p]),
     ("faf_cuda_get_stream", ctypes.c_void_p, [TP]),
+    ("faf_cuda_wait_status", ctypes.c_int, [TP]),
     ("faf_cuda_synchronize", ctypes.c_int, [TP]),
     ("faf_cuda_execute_c2c_noalloc", ctypes.c_int,
      [TP] + [ctypes.c_void_p] * 4 + [ctypes.c_size_t]),

@@ -624,6 +624,23 @@ extern "C" int faf_cuda_tc_status(const faf_transform* t) {
     return v ? 1 : 0;
 }
 
+extern "C" int faf_cuda_wait_status(const faf_transform* t) {
+    DevicePlan* p = plan_of(t);
+    if (!p) return fail("faf_cuda_wait_status: transform has no CUDA plan");
+    int v = 0, w = 0;
+    cudaError_t e = cudaStreamSynchronize(p->stream);
+    if (e == cudaSuccess && p->d_wait_err)
+        e = cudaMemcpy(&v, p->d_wait_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && p->d_tc_err)
+        e = cudaMemcpy(&w, p->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "faf_cuda_wait_status");
+    // nested plans (four-step factors, inner transforms) report through theirs
+    int rc = (v || w) ? 1 : 0;
+    if (!rc && t->inner && plan_of(t->inner)) rc = faf_cuda_wait_status(t->inner) == 1;
+    if (!rc && t->inner_inv && plan_of(t->inner_inv)) rc = faf_cuda_wait_status(t->inner_inv) == 1;
+    return rc;
+}
+
 extern "C" const char* faf_cuda_plan_kind(const faf_transform* t) {
     DevicePlan* p = plan_of(t);
     if (!p) return nullptr;

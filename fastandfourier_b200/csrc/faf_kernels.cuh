@@ -15,7 +15,7 @@ struct Geometry {
     int G;          // transforms per CTA
     int threads;    // G * T
     size_t smem;    // dynamic shared memory bytes
-    bool staged = false;  // power-of-two real-input kernels: cp.async input staging
+    int ring = 0;   // power-of-two real-input kernels: input ring slots (0: direct loads)
 };
 
 // Spectral op codes used inside the fused pipeline kernel.
@@ -65,6 +65,7 @@ struct RealArgs {  // R2C / C2R / pipeline / STFT
     // pipeline
     int nops;
     PipeOp ops[kMaxOps];
+    int* err;             // bit 1 set when a bounded wait of the kernel ran out
 };
 
 struct ConvArgs {  // Rader (prime n) and Bluestein (any n)

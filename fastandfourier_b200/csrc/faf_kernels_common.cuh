@@ -196,6 +196,23 @@ struct HermSink {  // split or interleaved Hermitian output
     }
 };
 
+// The two layouts of HermSink as separate types, for kernels that branch
+// once per transform instead of once per store.
+struct HermSplit {
+    float* re;
+    float* im;
+    __device__ __forceinline__ void put(int k, float r, float i) const {
+        __stcs(re + k, r);
+        __stcs(im + k, i);
+    }
+};
+struct HermInter {
+    float2* p;
+    __device__ __forceinline__ void put(int k, float r, float i) const {
+        __stcs(p + k, make_float2(r, i));
+    }
+};
+
 template <int E, class Src>
 __device__ __forceinline__ void r2c_body(const Shape& S, const Group& q,
                                          const float2* __restrict__ tw,

@@ -1,6 +1,7 @@
 // faf_plan.cu -- planner: radix programs, FP64 tables, launch geometry and
 // device-pointer execution for every plan kind.
 #include "faf_plan.h"
+#include "faf_ring.cuh"
 
 #include <cuda_fp16.h>
 
@@ -17,6 +18,7 @@ namespace {
 
 constexpr int kE = 16;                        // values per thread per stage
 constexpr size_t kMaxSmem = 227 * 1024;       // dynamic shared memory per CTA
+constexpr size_t kRingStatic = 1024;          // static shared memory of a ring kernel, rounded up
 constexpr int kTargetThreads = 256;
 
 template <class T>
@@ -228,20 +230,19 @@ void free_size(FftSize& s) {
 }
 
 // Geometry of the compile-time kernels: interleaved float2 workspace with one
-// pad element per 16 (plane2), T = n / 16 threads per transform, about 512
-// threads per CTA.
-fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, bool staged,
+// pad element per 16 (plane2), T = n / 16 threads per transform, about
+// `target_threads` threads per CTA.  With ring > 0 (and n >= 512), the shared
+// memory left after the workspaces holds up to `ring` input ring slots (n
+// float2 each, at most fafct::kRingMax); fewer than 2 slots means no ring.
+fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int ring,
                            int target_threads) {
     fafk::Geometry g;
     g.E = kE;
     const int T = s.n / 16;
-    // same layout as k_pot2.cu: even2(plane2(slots)) [+ n] float2 per group
+    // same layout as k_pot2.cu: even2(plane2(slots)) float2 per group
     const int plane2 = (slots - 1) + ((slots - 1) >> 4) + 1;
     const size_t table = fafk::pot2_table_smem(s.ct_log2);
-    size_t per = (size_t)((plane2 + 1) & ~1) * sizeof(float2);
-    // staging adds n float2 per group; drop it when one group no longer fits
-    if (staged && per + (size_t)s.n * sizeof(float2) + table > kMaxSmem) staged = false;
-    if (staged) per += (size_t)s.n * sizeof(float2);
+    const size_t per = (size_t)((plane2 + 1) & ~1) * sizeof(float2);
     int target = target_threads;
     if (const char* env = std::getenv("FAF_CUDA_CTA_THREADS")) target = std::max(1, atoi(env));
     int G = std::max(1, target / T);
@@ -252,7 +253,21 @@ fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, bool st
     g.G = G;
     g.threads = G * T;
     g.smem = (size_t)G * per;
-    g.staged = staged;
+    // The ring's consumers wait on other groups' progress, which needs every
+    // group in warps of its own (T >= 32): groups sharing a warp synchronise
+    // with warp barriers across the whole warp.
+    if (ring > 0 && T >= 32) {
+        const size_t slot = (size_t)s.n * sizeof(float2);
+        const size_t used = g.smem + table + kRingStatic;
+        int K = used < kMaxSmem ? (int)((kMaxSmem - used) / slot) : 0;
+        // FAF_CUDA_RING=k: k slots where they fit (k < 2: no ring)
+        const char* env = std::getenv("FAF_CUDA_RING");
+        K = std::min({K, env ? atoi(env) : ring, fafct::kRingMax});
+        if (K >= 2) {
+            g.ring = K;
+            g.smem += (size_t)K * slot;
+        }
+    }
     return g;
 }
 
@@ -269,19 +284,13 @@ fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long
     return g;
 }
 
-// cp.async staging of a real input needs every transform start 16-byte
-// aligned: base address and distance (floats) a multiple of 4.
-static bool stage_ok(const float* x, long long dist) {
+// Bulk copies of a real input into the ring need every transform start
+// 16-byte aligned: base address and distance (floats) a multiple of 4.
+// FAF_CUDA_NO_STAGING=1 turns the ring off (direct loads).
+static bool ring_ok(const float* x, long long dist) {
     const char* env = std::getenv("FAF_CUDA_NO_STAGING");
     if (env && env[0] == '1') return false;
     return ((unsigned long long)(size_t)x % 16 == 0) && (dist % 4 == 0);
-}
-
-// FAF_CUDA_STAGING=1 turns input staging on (the R2C and pipeline kernels
-// default to off).
-static bool stage_env() {
-    const char* env = std::getenv("FAF_CUDA_STAGING");
-    return env && env[0] == '1';
 }
 
 // ---------------------------------------------------------------------------
@@ -293,6 +302,12 @@ static DevicePlan* new_plan(Kind k, int n) {
     p->kind = k;
     p->n = n;
     cudaGetDevice(&p->device);
+    // bounded-wait flag of the kernels that wait on copies (left NULL if the
+    // allocation fails: those kernels then only skip the report)
+    if (cudaMalloc(&p->d_wait_err, sizeof(int)) == cudaSuccess)
+        cudaMemset(p->d_wait_err, 0, sizeof(int));
+    else
+        p->d_wait_err = nullptr, cudaGetLastError();
     return p;
 }
 
@@ -312,6 +327,7 @@ void plan_free(DevicePlan* p) {
     cudaFree(p->d_stw64);
     cudaFree(p->d_tcB);
     cudaFree(p->d_tc_err);
+    cudaFree(p->d_wait_err);
     cudaFree(p->d_stage);
     cudaFree(p->d_scratch);
     cudaFree(p->d_work);
@@ -753,6 +769,7 @@ static fafk::RealArgs real_args(DevicePlan* p, long long batch) {
     a.batch = batch;
     a.scale = p->scale;
     a.stw = p->d_stw;
+    a.err = p->d_wait_err;
     return a;
 }
 
@@ -766,13 +783,14 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
         return run_large(p, 1, &a, batch, st);
     }
     const int slots = p->inner.n + 1;
-    // measured on B200 (n = 4096, batch 8192): 1024-thread CTAs without
-    // input staging beat staged 512-thread CTAs (2900 vs 2580 GB/s)
+    // measured on B200 (n = 4096, batch 8192): 8 groups of 128 threads with
+    // a 4-slot input ring (as many slots as fit), 61 us per launch against 70
+    // with direct loads
     if (p->inner.ct_log2)
-        return fafk::launch_pot2(1, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch,
-                                             stage_env() && stage_ok(x, in_dist), 1024),
-                                 st);
+        return fafk::launch_pot2(
+            1, p->inner.ct_log2, p->inner.d_tws, &a,
+            geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? fafct::kRingMax : 0, 1024),
+            st);
     return fafk::launch_r2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);
 }
@@ -808,12 +826,15 @@ cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long bat
         return run_large(p, 3, &a, batch, st);
     }
     const int slots = p->inner.n + 1;
+    // measured on B200 (n = 4096, batch 8192): the two-FFT kernel is bound by
+    // issue, not by its loads; a 2-slot ring gains 2 % over direct loads and
+    // 3 or 4 slots lose 3 % (a larger shared carve-out leaves less L1 for
+    // the spectrum and super-twiddle tables)
     if (p->inner.ct_log2)
-        // measured on B200 (n = 4096, batch 8192): the two-FFT pipeline runs
-        // best without input staging in 1024-thread CTAs (1816 GB/s against
-        // 1699 at 512 and 1686 at 256)
         return fafk::launch_pot2(3, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch, stage_env(), 1024), st);
+                                 geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? 2 : 0,
+                                             1024),
+                                 st);
     return fafk::launch_pipeline(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                                  p->inner.d_tw, a, st);
 }
@@ -927,7 +948,6 @@ static fafk::Geometry geometry64(const FftSize& s, int slots, long long batch) {
     g.G = G;
     g.threads = G * s.T;
     g.smem = (size_t)G * per;
-    g.staged = false;
     return g;
 }
 

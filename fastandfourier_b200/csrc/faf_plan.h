@@ -40,7 +40,7 @@ bool build_size(int n, FftSize& out, std::string& err);
 void free_size(FftSize& s);
 int plane_floats(int slots);
 fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long batch);
-fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, bool staged = false,
+fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int ring = 0,
                            int target_threads = 512);
 
 enum class Kind {
@@ -87,6 +87,7 @@ struct DevicePlan {
     bool tc = false;
     void* d_tcB = nullptr;
     int* d_tc_err = nullptr;     // set by a kernel whose MMA wait ran out
+    int* d_wait_err = nullptr;   // set by a kernel whose input-ring wait ran out
     int win = 0, hop = 0;
     // launch state
     cudaStream_t stream = nullptr;  // 0 = legacy default stream

@@ -235,13 +235,14 @@ __device__ __forceinline__ void ct_fft(int t, float2* ws, const float2* __restri
 
 // Every stage but the last, from a global source; the workspace holds the
 // last stage's input when it returns (synchronised).
-template <int N, bool TWS_SMEM, class Src, class Sync>
+template <int N, bool TWS_SMEM, class Src, class Sync, class Hook = NoHook>
 __device__ __forceinline__ void ct_fft_but_last(int t, float2* ws, const float2* __restrict__ tws,
-                                                const Src& src, const Sync& sync) {
+                                                const Src& src, const Sync& sync,
+                                                const Hook& hook = Hook()) {
     float xr[16], xi[16];
     if constexpr (!Src::kSmem) sync();
-    ct_run<N, 0, TWS_SMEM, Src, SmemC, Sync, NoHook, true>(xr, xi, t, ws, tws, src, SmemC{ws},
-                                                           sync, NoHook());
+    ct_run<N, 0, TWS_SMEM, Src, SmemC, Sync, Hook, true>(xr, xi, t, ws, tws, src, SmemC{ws}, sync,
+                                                         hook);
 }
 
 // The last stage of an N-point transform whose last radix is 8 (two
@@ -309,22 +310,9 @@ __device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
     }
 }
 
-// ---- asynchronous input staging (cp.async, 16-byte chunks) ---------------
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-}
-
-// Staged input in shared memory, linear (no padding).  It is a different
-// buffer from the workspace, so the first stage needs no read/write barrier
-// (kSmem = false); the barrier at the start of ct_fft publishes the copies.
+// Input landed in shared memory (a ring slot, linear, no padding).  It is a
+// different buffer from the workspace, so the first stage needs no read/write
+// barrier (kSmem = false).
 struct StageSrc {
     const float2* s;
     static constexpr bool kSmem = false;

@@ -13,8 +13,9 @@ using fafct::plane2;
 
 // Shared-memory layout of one CTA:
 //   [twiddle table, if it fits 32 KB] [group 0 workspace] [group 1 ...] ...
+//   [input ring slots, kernels that land their input by bulk copy]
 // Every region is a whole number of 16-byte units (an even float2 count):
-// cp.async needs 16-byte aligned shared-memory destinations.
+// bulk copies need 16-byte aligned shared-memory destinations.
 __host__ __device__ constexpr int even2(int x) { return (x + 1) & ~1; }
 
 template <int N>
@@ -23,20 +24,18 @@ struct CtCfg {
     static constexpr int TWN = TW_SMEM ? even2(P2<N>::TW > 0 ? P2<N>::TW : 1) : 0;
 };
 
-// float2 units of one group: workspace (+ input staging)
-__host__ __device__ constexpr int group_stride(int n, int slots, bool staged) {
-    return even2(plane2(slots)) + (staged ? n : 0);
+// float2 units of one group's workspace
+__host__ __device__ constexpr int group_stride(int n, int slots) {
+    return (void)n, even2(plane2(slots));
 }
 
 template <int N>
 struct CtGroup {
     int g, t;
     float2* ws;
-    float2* stage;  // per-group input staging (N float2), when the kernel stages
     const float2* tw;
     fafct::GroupSync sync;
-    __device__ __forceinline__ CtGroup(float2* sm, int slots, const float2* __restrict__ gtw,
-                                       bool staged = false) {
+    __device__ __forceinline__ CtGroup(float2* sm, int slots, const float2* __restrict__ gtw) {
         constexpr int T = P2<N>::T;
         g = threadIdx.x / T;
         t = threadIdx.x % T;
@@ -46,8 +45,7 @@ struct CtGroup {
         } else {
             tw = gtw;
         }
-        ws = sm + CtCfg<N>::TWN + (size_t)g * group_stride(N, slots, staged);
-        stage = ws + even2(plane2(slots));
+        ws = sm + CtCfg<N>::TWN + (size_t)g * group_stride(N, slots);
         sync = fafct::GroupSync::make(g, T);
         // publish the twiddle table to the whole CTA once
         if constexpr (CtCfg<N>::TW_SMEM) __syncthreads();
@@ -56,6 +54,12 @@ struct CtGroup {
 
 template <int N>
 constexpr bool kTw = CtCfg<N>::TW_SMEM;
+
+// First ring slot behind the G group workspaces.
+template <int N>
+__device__ __forceinline__ float2* ring_base(float2* sm, int G, int slots) {
+    return sm + CtCfg<N>::TWN + (size_t)G * group_stride(N, slots);
+}
 
 // Persistent loop over transform groups; uniform across the CTA.
 #define CT_FOR_GROUPS(G, batch)                                                          \

@@ -11,6 +11,7 @@
 #include "faf_kernels_common.cuh"
 #include "faf_pot2.cuh"
 #include "faf_pot2_group.cuh"
+#include "faf_ring.cuh"
 
 namespace fafk {
 
@@ -20,27 +21,39 @@ using fafct::SmemCConj;
 using fafct::ct_fft;
 using fafct::plane2;
 
-// Prefetch of one real signal (2N floats, 16-byte aligned) into the group's
-// staging buffer: N/2 chunks of 16 bytes, 8 per thread.
-template <int N>
-__device__ __forceinline__ void prefetch_real(float2* stage, const float* x, int t, bool live) {
-    if (live) {
-#pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int c = t + j * P2<N>::T;
-            fafct::cp_async16(stage + 2 * c, x + 4 * c);
-        }
+// Issues the copy of the transform `src` (sequence s of the CTA's ring) once
+// the group's first stage has read its own slot; one thread of the group.
+struct RingHook {
+    fafct::Ring r;
+    int slot, use;    // the slot just read, and the number of the copy to issue into it
+    const void* src;  // NULL: nothing left to load
+    unsigned bytes;
+    int t;
+    __device__ __forceinline__ void operator()() const {
+        if (t == 0 && src) r.issue(slot, use, src, bytes);
     }
-    fafct::cp_async_commit();
+};
+
+// The ring of a real-input kernel: one slot per transform input (2N floats).
+template <int N>
+__device__ __forceinline__ fafct::Ring real_ring(fafct::RingCtl* ctl, float2* sm, int G, int K,
+                                                 const RealArgs& a) {
+    return fafct::ring_start(
+        ctl, ring_base<N>(sm, G, N + 1), K, N, G, a.batch,
+        [&](long long b) { return (const void*)(a.in_a + b * a.in_dist); }, N * 8u);
 }
 
-template <int N>
-struct PrefetchNext {
-    float2* stage;
-    const float* x;  // next signal's input, or NULL
-    int t;
-    __device__ __forceinline__ void operator()() const { prefetch_real<N>(stage, x, t, x != nullptr); }
-};
+// Waits for the group's current transform b (cursor c) and returns the hook
+// that loads transform b + dnext (sequence s + K) into the same slot.
+__device__ __forceinline__ RingHook ring_next(const fafct::Ring& R, const fafct::RingCursor& c,
+                                              long long b, int dnext, bool live, const float* in,
+                                              long long dist, long long batch, unsigned bytes,
+                                              int t, int* err) {
+    if (live && !R.wait(c) && t == 0) R.fail(err);
+    const long long bn = b + dnext;
+    return RingHook{R, c.slot, c.use + 1, (live && bn < batch) ? in + bn * dist : nullptr,
+                    bytes, t};
+}
 
 template <int N>
 __global__ void __launch_bounds__(1024) k2_c2c(const float2* __restrict__ tws, const C2CArgs a,
@@ -82,55 +95,84 @@ __device__ __forceinline__ void ct_r2c_post(int t, const SmemC& mid,
     }
 }
 
-template <int N, bool ASYNC>
+// RING: inputs land in the CTA's ring by bulk copy (in_a 16-byte aligned,
+// in_dist a multiple of 4); otherwise the first stage loads them.
+template <int N, bool RING>
 __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, const RealArgs a,
-                                               int G, bool vec) {
+                                               int G, bool vec, int K) {
     extern __shared__ float4 smem4[];
-    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws, ASYNC);
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    CtGroup<N> q(sm, N + 1, tws);
     const SmemC mid{q.ws};
     const int fpe = a.interleaved ? 2 : 1;
-    if constexpr (ASYNC) {
-        const long long b0 = (long long)blockIdx.x * G + q.g;
-        prefetch_real<N>(q.stage, a.in_a + b0 * a.in_dist, q.t, b0 < a.batch);
+    fafct::Ring R{};
+    if constexpr (RING) {
+        __shared__ fafct::RingCtl ctl;
+        R = real_ring<N>(&ctl, sm, G, K, a);
     }
+    fafct::RingCursor c{};
+    int dnext = 0;
+    if constexpr (RING) {
+        c = R.cursor(q.g);
+        dnext = R.next_offset(q.g);
+    }
+    bool first = true;
     CT_FOR_GROUPS(G, a.batch) {
+        if constexpr (RING) {
+            if (!first) R.advance(c);
+            first = false;
+        }
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        if constexpr (ASYNC) {
-            const long long bn = (grp_ + gridDim.x) * G + q.g;
-            const float* xn = bn < a.batch ? a.in_a + bn * a.in_dist : nullptr;
-            fafct::cp_async_wait_all();
-            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{q.stage}, mid, q.sync,
-                              PrefetchNext<N>{q.stage, xn, q.t});
-        } else if constexpr (fafct::LastPairs<N>::ok) {
+        if constexpr (fafct::LastPairs<N>::ok) {
             // last stage fused with the post-pass: no workspace round trip
-            fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw,
-                                              RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
-                                              q.sync);
+            if constexpr (RING) {
+                const RingHook hook =
+                    ring_next(R, c, b, dnext, live, a.in_a, a.in_dist, a.batch, N * 8u, q.t,
+                              a.err);
+                fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)},
+                                                  q.sync, hook);
+            } else {
+                fafct::ct_fft_but_last<N, kTw<N>>(
+                    q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, q.sync);
+            }
             if (live) {
                 const long long oo = bi * a.out_dist * fpe;
-                const HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo,
-                                   a.interleaved};
                 const float sc = a.scale;
                 const float2* __restrict__ stw = a.stw;
-                fafct::ct_last_pairs<N, kTw<N>>(
-                    q.t, q.ws, q.tw,
-                    [&](cf z) {
-                        out.put(0, (z.x + z.y) * sc, 0.f);
-                        out.put(N, (z.x - z.y) * sc, 0.f);
-                    },
-                    [&](int k, cf zk, cf zn) {
-                        cf Xk, Xnk;
-                        r2c_pair(zk, zn, __ldg(&stw[k - 1]), Xk, Xnk);
-                        if (k != N - k) out.put(k, Xk.x * sc, Xk.y * sc);
-                        out.put(N - k, Xnk.x * sc, Xnk.y * sc);
-                    });
+                // one branch per transform on the layout: a per-store branch
+                // costs the fused stage registers it does not have
+                auto post = [&](const auto& out) {
+                    fafct::ct_last_pairs<N, kTw<N>>(
+                        q.t, q.ws, q.tw,
+                        [&](cf z) {
+                            out.put(0, (z.x + z.y) * sc, 0.f);
+                            out.put(N, (z.x - z.y) * sc, 0.f);
+                        },
+                        [&](int k, cf zk, cf zn) {
+                            cf Xk, Xnk;
+                            r2c_pair(zk, zn, __ldg(&stw[k - 1]), Xk, Xnk);
+                            if (k != N - k) out.put(k, Xk.x * sc, Xk.y * sc);
+                            out.put(N - k, Xnk.x * sc, Xnk.y * sc);
+                        });
+                };
+                if (a.interleaved)
+                    post(HermInter{reinterpret_cast<float2*>(a.out_a + oo)});
+                else
+                    post(HermSplit{a.out_a + oo, a.out_b + oo});
             }
             continue;
         } else {
-            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
-                              mid, q.sync);
+            if constexpr (RING) {
+                const RingHook hook =
+                    ring_next(R, c, b, dnext, live, a.in_a, a.in_dist, a.batch, N * 8u, q.t,
+                              a.err);
+                ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)}, mid, q.sync, hook);
+            } else {
+                ct_fft<N, kTw<N>>(q.t, q.ws, q.tw,
+                                  RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid, q.sync);
+            }
         }
         q.sync();
         if (live) {
@@ -139,6 +181,7 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
             ct_r2c_post<N>(q.t, mid, a.stw, out, a.scale);
         }
     }
+    if constexpr (RING) fafct::ring_drain(R);
 }
 
 template <int N>
@@ -264,39 +307,58 @@ __device__ __forceinline__ void pipe_middle_fused(int t, float2* ws, const float
         });
 }
 
-template <int N, bool ASYNC>
+template <int N, bool RING>
 __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ tws,
-                                                    const RealArgs a, int G, bool vec) {
+                                                    const RealArgs a, int G, bool vec, int K) {
     extern __shared__ float4 smem4[];
-    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws, ASYNC);
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    CtGroup<N> q(sm, N + 1, tws);
     const SmemC mid{q.ws};
-    if constexpr (ASYNC) {
-        const long long b0 = (long long)blockIdx.x * G + q.g;
-        prefetch_real<N>(q.stage, a.in_a + b0 * a.in_dist, q.t, b0 < a.batch);
+    fafct::Ring R{};
+    if constexpr (RING) {
+        __shared__ fafct::RingCtl ctl;
+        R = real_ring<N>(&ctl, sm, G, K, a);
     }
+    fafct::RingCursor c{};
+    int dnext = 0;
+    if constexpr (RING) {
+        c = R.cursor(q.g);
+        dnext = R.next_offset(q.g);
+    }
+    bool first = true;
     CT_FOR_GROUPS(G, a.batch) {
+        if constexpr (RING) {
+            if (!first) R.advance(c);
+            first = false;
+        }
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        if constexpr (ASYNC) {
-            const long long bn = (grp_ + gridDim.x) * G + q.g;
-            const float* xn = bn < a.batch ? a.in_a + bn * a.in_dist : nullptr;
-            fafct::cp_async_wait_all();
-            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{q.stage}, mid, q.sync,
-                              PrefetchNext<N>{q.stage, xn, q.t});
-        } else if constexpr (fafct::LastPairs<N>::ok) {
-            fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw,
-                                              RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
-                                              q.sync);
+        if constexpr (fafct::LastPairs<N>::ok) {
+            if constexpr (RING) {
+                const RingHook hook =
+                    ring_next(R, c, b, dnext, live, a.in_a, a.in_dist, a.batch, N * 8u, q.t,
+                              a.err);
+                fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)},
+                                                  q.sync, hook);
+            } else {
+                fafct::ct_fft_but_last<N, kTw<N>>(
+                    q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, q.sync);
+            }
             if (ops_single_mul(a))
                 pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsMul1{&a.ops[0]});
             else
                 pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsAny{&a});
         } else {
-            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec},
-                              mid, q.sync);
-        }
-        if constexpr (!fafct::LastPairs<N>::ok || ASYNC) {
+            if constexpr (RING) {
+                const RingHook hook =
+                    ring_next(R, c, b, dnext, live, a.in_a, a.in_dist, a.batch, N * 8u, q.t,
+                              a.err);
+                ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)}, mid, q.sync, hook);
+            } else {
+                ct_fft<N, kTw<N>>(q.t, q.ws, q.tw,
+                                  RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid, q.sync);
+            }
             q.sync();
             if (ops_single_mul(a))
                 pipe_middle<N>(q.t, mid, a.stw, OpsMul1{&a.ops[0]});
@@ -307,6 +369,7 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
         ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
                           RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec}, q.sync);
     }
+    if constexpr (RING) fafct::ring_drain(R);
 }
 
 // ---------------------------------------------------------------------------
@@ -332,6 +395,11 @@ static unsigned persistent_grid(K kernel, const Geometry& g, long long batch) {
     return (unsigned)std::max(1LL, std::min(groups, cap));
 }
 
+// The ring needs groups of at least one warp (T = N / 16 >= 32); shorter
+// lengths are built without it.
+template <int N>
+constexpr bool kRingN = N >= 512;
+
 template <int N>
 static size_t tw_bytes() {
     return (size_t)CtCfg<N>::TWN * sizeof(float2);
@@ -351,14 +419,14 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     }
     case 1: {
         const RealArgs& a = *(const RealArgs*)args;
-        if (g.staged) {
-            if ((e = prep(k2_r2c<N, true>, g.smem)) != cudaSuccess) return e;
-            k2_r2c<N, true><<<persistent_grid(k2_r2c<N, true>, g, a.batch), g.threads, g.smem,
-                              st>>>(tws, a, g.G, true);
+        if (kRingN<N> && g.ring) {
+            if ((e = prep(k2_r2c<N, kRingN<N>>, g.smem)) != cudaSuccess) return e;
+            k2_r2c<N, kRingN<N>><<<persistent_grid(k2_r2c<N, kRingN<N>>, g, a.batch), g.threads,
+                                   g.smem, st>>>(tws, a, g.G, true, g.ring);
         } else {
             if ((e = prep(k2_r2c<N, false>, g.smem)) != cudaSuccess) return e;
             k2_r2c<N, false><<<persistent_grid(k2_r2c<N, false>, g, a.batch), g.threads, g.smem,
-                               st>>>(tws, a, g.G, vec_ok(a.in_a, a.in_dist));
+                               st>>>(tws, a, g.G, vec_ok(a.in_a, a.in_dist), 0);
         }
         break;
     }
@@ -372,14 +440,14 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     case 3: {
         const RealArgs& a = *(const RealArgs*)args;
         const bool vec = vec_ok(a.in_a, a.in_dist) && vec_ok(a.out_a, a.out_dist);
-        if (g.staged) {
-            if ((e = prep(k2_pipeline<N, true>, g.smem)) != cudaSuccess) return e;
-            k2_pipeline<N, true><<<persistent_grid(k2_pipeline<N, true>, g, a.batch), g.threads,
-                                   g.smem, st>>>(tws, a, g.G, vec);
+        if (kRingN<N> && g.ring) {
+            if ((e = prep(k2_pipeline<N, kRingN<N>>, g.smem)) != cudaSuccess) return e;
+            k2_pipeline<N, kRingN<N>><<<persistent_grid(k2_pipeline<N, kRingN<N>>, g, a.batch),
+                                        g.threads, g.smem, st>>>(tws, a, g.G, vec, g.ring);
         } else {
             if ((e = prep(k2_pipeline<N, false>, g.smem)) != cudaSuccess) return e;
             k2_pipeline<N, false><<<persistent_grid(k2_pipeline<N, false>, g, a.batch),
-                                    g.threads, g.smem, st>>>(tws, a, g.G, vec);
+                                    g.threads, g.smem, st>>>(tws, a, g.G, vec, 0);
         }
         break;
     }

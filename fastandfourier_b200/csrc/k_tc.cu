@@ -299,7 +299,7 @@ template <int N>
 constexpr size_t smem_bytes() {
     constexpr int G = kThreads / P2<N>::T;
     return (size_t)CtCfg<N>::TWN * sizeof(float2) +
-           (size_t)G * group_stride(N, N, false) * sizeof(float2) + kTailBytes;
+           (size_t)G * group_stride(N, N) * sizeof(float2) + kTailBytes;
 }
 
 template <int N>
@@ -308,14 +308,14 @@ __global__ void __launch_bounds__(kThreads, 1)
               int* err) {
     static_assert(P2<N>::N16 >= 1, "needs at least one radix-16 stage");
     constexpr int G = kThreads / P2<N>::T;
-    static_assert((size_t)G * group_stride(N, N, false) * sizeof(float2) >=
+    static_assert((size_t)G * group_stride(N, N) * sizeof(float2) >=
                       (size_t)kWarpgroups * 2 * kTileBytes,
                   "A tiles must fit in the workspace they alias");
     extern __shared__ float4 smem4[];
     float2* sm2 = reinterpret_cast<float2*>(smem4);
     CtGroup<N> q(sm2, N, tws);
     uint8_t* wsb = reinterpret_cast<uint8_t*>(sm2 + CtCfg<N>::TWN);
-    uint8_t* bsm = wsb + (size_t)G * group_stride(N, N, false) * sizeof(float2);
+    uint8_t* bsm = wsb + (size_t)G * group_stride(N, N) * sizeof(float2);
     uint64_t* bars = reinterpret_cast<uint64_t*>(bsm + kBBytes);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kWarpgroups);
     const int wg = threadIdx.x >> 7, warp = threadIdx.x >> 5;

@@ -40,6 +40,11 @@ const char *faf_cuda_plan_kind(const faf_transform *t);
  * completed, 1 if one ran out of its bound (the results are then invalid);
  * -1 if t is not a tensor-core plan.  Synchronises the plan's stream. */
 int faf_cuda_tc_status(const faf_transform *t);
+/* 0 if every bounded wait of this transform's kernels so far completed (the
+ * input ring's copy waits, tensor-core MMA waits), 1 if one ran out (the
+ * results of that launch are then invalid), -1 on error.  Synchronises the
+ * transform's stream. */
+int faf_cuda_wait_status(const faf_transform *t);
 /* Number of kernel launches the last execute on this thread made. */
 int faf_cuda_last_launches(void);
 

@@ -1,0 +1,86 @@
+"""The input landing ring of the power-of-two R2C and pipeline kernels (inputs
+land in shared-memory slots by bulk copy, a slot cycle ahead of use): parity
+against FP64 numpy over ragged batches and input distances, the direct-load
+path for distances the bulk copy cannot take, and a clean wait status."""
+import numpy as np
+import pytest
+
+from conftest import REL_L2_TOL, seeded
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(got, want):
+    return float(np.linalg.norm(got - want) / np.linalg.norm(want))
+
+
+def _strided(torch, x, dist):
+    """(batch, n) rows placed `dist` floats apart in one device buffer."""
+    b, n = x.shape
+    buf = torch.zeros(b * dist, dtype=torch.float32, device="cuda")
+    buf.view(b, dist)[:, :n] = torch.from_numpy(x).cuda()
+    return buf
+
+
+@pytest.mark.parametrize("n", [64, 1024, 4096, 8192])
+@pytest.mark.parametrize("batch", [1, 5, 1187, 8192 + 13])
+def test_r2c_ring_batches(cuda, n, batch):
+    import fastandfourier_b200 as F
+    torch = cuda
+    x = seeded(n + batch).standard_normal((batch, n)).astype(np.float32)
+    t = F.Transform.rfft(n)
+    Xr, Xi = t.r2c(torch.from_numpy(x).cuda())
+    want = np.fft.rfft(x.astype(np.float64), axis=-1)
+    assert rel(Xr.cpu().numpy() + 1j * Xi.cpu().numpy(), want) <= REL_L2_TOL
+    assert t.wait_status() == 0
+
+
+@pytest.mark.parametrize("dist_pad", [1, 2, 4, 12])
+def test_r2c_ring_and_direct_distances(cuda, dist_pad):
+    """dist % 4 == 0 takes the ring, other distances the direct loads."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n, batch = 4096, 700
+    dist = n + dist_pad
+    x = seeded(dist).standard_normal((batch, n)).astype(np.float32)
+    buf = _strided(torch, x, dist)
+    nb = n // 2 + 1
+    Xr = torch.empty(batch * nb, device="cuda")
+    Xi = torch.empty(batch * nb, device="cuda")
+    t = F.Transform.rfft(n)
+    t.execute_batched(F._buf(Xr, Xi, nb, F.L_HERMITIAN), F._buf(buf, None, n, F.L_REAL), batch,
+                      in_dist=dist, out_dist=nb)
+    got = Xr.cpu().numpy().reshape(batch, nb) + 1j * Xi.cpu().numpy().reshape(batch, nb)
+    assert rel(got, np.fft.rfft(x.astype(np.float64), axis=-1)) <= REL_L2_TOL
+    assert t.wait_status() == 0
+
+
+@pytest.mark.parametrize("batch", [3, 640, 8192 + 7])
+def test_pipeline_ring_batches(cuda, batch):
+    import fastandfourier_b200 as F
+    torch = cuda
+    n, nb = 4096, 2049
+    rng = seeded(batch)
+    x = rng.standard_normal((batch, n)).astype(np.float32)
+    m = rng.uniform(0, 1, nb).astype(np.float32)
+    t = F.Transform.chirp("(pipeline (rfft :size 4096) (mul-spectrum) (irfft))")
+    hm = torch.from_numpy(m).cuda()
+    hz = torch.zeros(nb, device="cuda")
+    t.bind(hm, hz, nb)
+    y = t.pipeline(torch.from_numpy(x).cuda()).cpu().numpy()
+    want = np.fft.irfft(np.fft.rfft(x.astype(np.float64), axis=-1) * m, n=n, axis=-1)
+    assert rel(y, want) <= REL_L2_TOL
+    assert t.wait_status() == 0
+
+
+def test_ring_off_matches_ring_on(cuda, monkeypatch):
+    """FAF_CUDA_NO_STAGING=1 (direct loads) gives bit-identical results: the
+    ring changes where the input comes from, not the arithmetic."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    x = torch.from_numpy(seeded(77).standard_normal((333, 4096)).astype(np.float32)).cuda()
+    t = F.Transform.rfft(4096)
+    a_re, a_im = t.r2c(x)
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    b_re, b_im = t.r2c(x)
+    assert torch.equal(a_re, b_re) and torch.equal(a_im, b_im)
