@@ -104,6 +104,20 @@ struct FrameSrc {
     }
 };
 
+// The same frame landed in shared memory (a ring slot holding its first
+// `win` samples) with the window in shared memory too.
+struct FrameStageSrc {
+    const float2* s;  // slot: x[2i], x[2i+1] as float2 i
+    const float2* w;  // window, the same pairing
+    int win;          // even
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ cf get(int i) const {
+        if (2 * i >= win) return cf{0.f, 0.f};
+        const float2 v = s[i], u = w[i];
+        return cf{v.x * u.x, v.y * u.y};
+    }
+};
+
 // y[2k] = Re z, y[2k+1] = Im z, with the conjugation of an inverse FFT undone
 // (C2R unpack, reference src/faf_rfft.c:392-395).
 struct RealPairSink {

@@ -233,9 +233,10 @@ void free_size(FftSize& s) {
 // pad element per 16 (plane2), T = n / 16 threads per transform, about
 // `target_threads` threads per CTA.  With ring > 0 (and n >= 512), the shared
 // memory left after the workspaces holds up to `ring` input ring slots (n
-// float2 each, at most fafct::kRingMax); fewer than 2 slots means no ring.
+// float2 each, at most fafct::kRingMax) and `ring_extra` bytes behind them;
+// fewer than 2 slots means no ring.
 fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int ring,
-                           int target_threads) {
+                           int target_threads, size_t ring_extra) {
     fafk::Geometry g;
     g.E = kE;
     const int T = s.n / 16;
@@ -258,14 +259,14 @@ fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int rin
     // with warp barriers across the whole warp.
     if (ring > 0 && T >= 32) {
         const size_t slot = (size_t)s.n * sizeof(float2);
-        const size_t used = g.smem + table + kRingStatic;
+        const size_t used = g.smem + table + kRingStatic + ring_extra;
         int K = used < kMaxSmem ? (int)((kMaxSmem - used) / slot) : 0;
         // FAF_CUDA_RING=k: k slots where they fit (k < 2: no ring)
         const char* env = std::getenv("FAF_CUDA_RING");
         K = std::min({K, env ? atoi(env) : ring, fafct::kRingMax});
         if (K >= 2) {
             g.ring = K;
-            g.smem += (size_t)K * slot;
+            g.smem += (size_t)K * slot + ring_extra;
         }
     }
     return g;
@@ -282,6 +283,14 @@ fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long
     g.threads = G * s.T;
     g.smem = (size_t)G * per;
     return g;
+}
+
+// Input ring slots of the STFT kernel (FAF_CUDA_STFT_RING overrides).
+// Measured on B200 (Hann 1024 / hop 256, 64 x 2^18 samples): 4 slots 129.5
+// us, 8 slots 131.4, 2 slots 171.7, direct loads 137.0.
+static int stft_ring() {
+    const char* env = std::getenv("FAF_CUDA_STFT_RING");
+    return env ? atoi(env) : 4;
 }
 
 // Bulk copies of a real input into the ring need every transform start
@@ -849,9 +858,15 @@ cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long 
     a.window = p->d_window; a.win = p->win; a.hop = p->hop;
     a.sig_len = sig_len; a.frames = frames;
     const int slots = p->inner.n + 1;
+    // frames land by bulk copy when every frame start is 16-byte aligned and
+    // the window is a whole number of 16-byte units
+    const bool ring = ring_ok(x, sig_len) && a.hop % 4 == 0 && a.win % 4 == 0;
     if (p->inner.ct_log2)
-        return fafk::launch_pot2(4, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch), st);
+        return fafk::launch_pot2(
+            4, p->inner.ct_log2, p->inner.d_tws, &a,
+            geometry_ct(p->inner, slots, batch, ring ? stft_ring() : 0, 512,
+                        ((size_t)a.win * sizeof(float) + 15) & ~(size_t)15),
+            st);
     return fafk::launch_stft(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                              p->inner.d_tw, a, st);
 }

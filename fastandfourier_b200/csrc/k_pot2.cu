@@ -44,15 +44,25 @@ __device__ __forceinline__ fafct::Ring real_ring(fafct::RingCtl* ctl, float2* sm
 }
 
 // Waits for the group's current transform b (cursor c) and returns the hook
-// that loads transform b + dnext (sequence s + K) into the same slot.
+// that loads transform b + dnext (sequence s + K) into the same slot;
+// src_of(bn) is transform bn's input.
+template <class SrcOf>
+__device__ __forceinline__ RingHook ring_next_of(const fafct::Ring& R, const fafct::RingCursor& c,
+                                                 long long b, int dnext, bool live,
+                                                 long long batch, const SrcOf& src_of,
+                                                 unsigned bytes, int t, int* err) {
+    if (live && !R.wait(c) && t == 0) R.fail(err);
+    const long long bn = b + dnext;
+    return RingHook{R, c.slot, c.use + 1, (live && bn < batch) ? src_of(bn) : nullptr, bytes, t};
+}
+
 __device__ __forceinline__ RingHook ring_next(const fafct::Ring& R, const fafct::RingCursor& c,
                                               long long b, int dnext, bool live, const float* in,
                                               long long dist, long long batch, unsigned bytes,
                                               int t, int* err) {
-    if (live && !R.wait(c) && t == 0) R.fail(err);
-    const long long bn = b + dnext;
-    return RingHook{R, c.slot, c.use + 1, (live && bn < batch) ? in + bn * dist : nullptr,
-                    bytes, t};
+    return ring_next_of(
+        R, c, b, dnext, live, batch, [&](long long bn) { return (const void*)(in + bn * dist); },
+        bytes, t, err);
 }
 
 template <int N>
@@ -184,21 +194,55 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
     if constexpr (RING) fafct::ring_drain(R);
 }
 
-template <int N>
+// RING: each frame's first `win` samples land in the ring by bulk copy
+// (frame starts 16-byte aligned, win a multiple of 4), the window is staged in
+// shared memory behind the ring; otherwise the first stage loads both.
+template <int N, bool RING>
 __global__ void __launch_bounds__(1024) k2_stft(const float2* __restrict__ tws, const RealArgs a,
-                                                int G) {
+                                                int G, int K) {
     extern __shared__ float4 smem4[];
-    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws);
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    CtGroup<N> q(sm, N + 1, tws);
     const SmemC mid{q.ws};
     const int fpe = a.interleaved ? 2 : 1;
+    auto frame = [&](long long b) {
+        const long long sig = b / a.frames, f = b - sig * a.frames;
+        return a.in_a + sig * a.sig_len + f * a.hop;
+    };
+    fafct::Ring R{};
+    fafct::RingCursor c{};
+    int dnext = 0;
+    const float2* wsm = nullptr;
+    if constexpr (RING) {
+        __shared__ fafct::RingCtl ctl;
+        float2* wbuf = ring_base<N>(sm, G, N + 1) + (size_t)K * N;
+        for (int i = threadIdx.x; i < a.win / 2; i += blockDim.x)
+            wbuf[i] = __ldg(reinterpret_cast<const float2*>(a.window) + i);
+        wsm = wbuf;  // published by the barrier in ring_start
+        R = fafct::ring_start(
+            &ctl, ring_base<N>(sm, G, N + 1), K, N, G, a.batch,
+            [&](long long b) { return (const void*)frame(b); }, (unsigned)a.win * 4u);
+        c = R.cursor(q.g);
+        dnext = R.next_offset(q.g);
+    }
+    bool first = true;
     CT_FOR_GROUPS(G, a.batch) {
         const long long b = grp_ * G + q.g;  // global frame index
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        const long long sig = bi / a.frames, f = bi - sig * a.frames;
-        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw,
-                          FrameSrc{a.in_a + sig * a.sig_len + f * a.hop, a.window, a.win, live},
-                          mid, q.sync);
+        if constexpr (RING) {
+            if (!first) R.advance(c);
+            first = false;
+            const RingHook hook =
+                ring_next_of(R, c, b, dnext, live, a.batch,
+                             [&](long long bn) { return (const void*)frame(bn); },
+                             (unsigned)a.win * 4u, q.t, a.err);
+            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, FrameStageSrc{R.slot_ptr(c), wsm, a.win}, mid,
+                              q.sync, hook);
+        } else {
+            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, FrameSrc{frame(bi), a.window, a.win, live}, mid,
+                              q.sync);
+        }
         q.sync();
         if (live) {
             const long long oo = bi * a.out_dist * fpe;
@@ -206,6 +250,7 @@ __global__ void __launch_bounds__(1024) k2_stft(const float2* __restrict__ tws, 
             ct_r2c_post<N>(q.t, mid, a.stw, out, a.scale);
         }
     }
+    if constexpr (RING) fafct::ring_drain(R);
 }
 
 template <int N>
@@ -453,9 +498,15 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     }
     case 4: {
         const RealArgs& a = *(const RealArgs*)args;
-        if ((e = prep(k2_stft<N>, g.smem)) != cudaSuccess) return e;
-        k2_stft<N><<<persistent_grid(k2_stft<N>, g, a.batch), g.threads, g.smem, st>>>(tws, a,
-                                                                                        g.G);
+        if (kRingN<N> && g.ring) {
+            if ((e = prep(k2_stft<N, kRingN<N>>, g.smem)) != cudaSuccess) return e;
+            k2_stft<N, kRingN<N>><<<persistent_grid(k2_stft<N, kRingN<N>>, g, a.batch),
+                                    g.threads, g.smem, st>>>(tws, a, g.G, g.ring);
+        } else {
+            if ((e = prep(k2_stft<N, false>, g.smem)) != cudaSuccess) return e;
+            k2_stft<N, false><<<persistent_grid(k2_stft<N, false>, g, a.batch), g.threads,
+                                g.smem, st>>>(tws, a, g.G, 0);
+        }
         break;
     }
     default:

@@ -84,3 +84,31 @@ def test_ring_off_matches_ring_on(cuda, monkeypatch):
     monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
     b_re, b_im = t.r2c(x)
     assert torch.equal(a_re, b_re) and torch.equal(a_im, b_im)
+
+
+@pytest.mark.parametrize("n,win,hop", [(1024, 1024, 256), (512, 400, 100), (2048, 2048, 512),
+                                       (1024, 1000, 250)])
+def test_stft_ring_matches_direct(cuda, monkeypatch, n, win, hop):
+    """STFT frames landed by bulk copy (aligned frame starts, win % 4 == 0)
+    equal the direct loads bit for bit; hop 250 (frame starts not 16-byte
+    aligned) takes the direct path both times.  Both match FP64 numpy."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    L = 40000
+    x = seeded(n + win + hop).standard_normal((3, L)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    t = F.Transform.stft(n, win=win, hop=hop)
+    a_re, a_im = t.stft_frames(xd)
+    assert t.wait_status() == 0
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    b_re, b_im = t.stft_frames(xd)
+    assert torch.equal(a_re, b_re) and torch.equal(a_im, b_im)
+    frames = 1 + (L - win) // hop
+    k = np.arange(win)
+    w = 0.5 * (1 - np.cos(2 * np.pi * k / (win - 1)))
+    idx = np.arange(frames)[:, None] * hop + k[None, :]
+    fr = np.zeros((3, frames, n))
+    fr[:, :, :win] = x.astype(np.float64)[:, idx] * w
+    want = np.fft.rfft(fr, axis=-1)
+    got = a_re.cpu().numpy() + 1j * a_im.cpu().numpy()
+    assert rel(got, want) <= REL_L2_TOL
