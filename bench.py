@@ -11,7 +11,7 @@ of the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload pipeline|r2c|c2c1024|c2c16384|c2c16384tc|c2c4096fp64|
-                                stft|istft|uneven|serve]
+                                stft|istft|cwt|uneven|serve]
 
 --workload serve replays a Poisson request trace (20k requests/s: 40% rfft
 of log-uniform sizes 256..65536 rounded to the recommended size, 30% the
@@ -84,6 +84,24 @@ WORKLOADS["c2c4096fp64"] = ("C2C n=4096 batch 4096 forward in FP64 (split planes
 WORKLOADS["istft"] = ("inverse STFT Hann 1024 hop 256: 64 signals x 1021 frames x 513 bins -> "
                       "2^18 samples, N(0,1) frames, seed 4", 1024, 64, None, None)
 
+# 60 rows: the row count of the reference's default bank (Morse 20/3, 10
+# voices, lowpass) at n = 4096; the rows themselves are synthetic here.
+CWT_ROWS = 60
+WORKLOADS["cwt"] = ("CWT filter bank n=4096: 256 signals x 60 rows (synthetic Gaussian bandpass "
+                    "bank, seed 6; the reference's default bank has 60 rows at this n), N(0,1) "
+                    "signals, seed 5", 4096, 256, 4 * 4096 * (1 + CWT_ROWS), None)
+
+
+def cwt_bank(rows=CWT_ROWS, n=4096, seed=6):
+    """Seeded Gaussian bandpass rows on geometric centres (an analytic
+    wavelet bank's shape: positive, one octave per 10 rows)."""
+    nb = n // 2 + 1
+    k = np.arange(nb)[None, :]
+    c = np.geomspace(2.0, 0.8 * nb, rows)[:, None]
+    g = np.random.default_rng(seed).uniform(0.8, 1.2, (rows, 1))
+    return (g * np.exp(-0.5 * ((k - c) / (0.2 * c + 1.0)) ** 2)).astype(np.float32)
+
+
 WORKLOADS["serve"] = ("serving trace: 4000 requests, Poisson 20k req/s (seed 4); 40% rfft "
                       "N log-uniform [256, 65536] -> recommended size, 30% notch pipeline "
                       "4096, 30% STFT Hann 1024 hop 256 over L log-uniform [2^16, 2^20]; "
@@ -125,6 +143,8 @@ def make_inputs(workload, batch):
     if workload == "stft":
         rng = np.random.default_rng(4)
         return [rng.standard_normal((batch, 1 << 18), dtype=np.float32)]
+    if workload == "cwt":
+        return [np.random.default_rng(5).standard_normal((batch, n), dtype=np.float32)]
     if workload == "uneven":
         total = sum(uneven_lengths(batch))
         rng = np.random.default_rng(2)
@@ -247,6 +267,8 @@ def build_transform(F, workload, torch):
         return F.Transform.fft(n, precision=F.PREC_FP64)
     if workload == "istft":
         return F.Transform.istft(1024, win=1024, hop=256)
+    if workload == "cwt":
+        return F.Transform.cwt(4096, cwt_bank())
     if workload.startswith("c2c"):
         return F.Transform.fft(n)
     if workload == "stft":
@@ -267,6 +289,8 @@ def run_step(F, t, workload, ins, outs, plain=False):
         t.stft_frames(ins[0], out_re=outs[0], out_im=outs[1])
     elif workload == "istft":
         t.istft_frames(ins[0], ins[1], out=outs[0])
+    elif workload == "cwt":
+        t.analyze(ins[0], out=outs[0])
     elif workload == "uneven":
         if hasattr(ins[0], "data_ptr"):
             t.execute(ins[0], ins[1], outs[0], outs[1], plain=plain)
@@ -306,6 +330,8 @@ def alloc_outputs(workload, batch, like, torch):
         return [mk((batch, F_, 513)), mk((batch, F_, 513))]
     if workload == "istft":
         return [mk((batch, 1 << 18))]
+    if workload == "cwt":
+        return [mk((batch, CWT_ROWS, n))]
     if workload == "uneven":
         total = sum(uneven_lengths(batch))
         return [mk((total,)), mk((total,))]
@@ -459,7 +485,8 @@ def run_ours(args, rank, world, local_rank):
                 "algorithmic_bytes_per_launch": nbytes,
                 "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
                            "uneven": "k_uneven_large", "c2c16384tc": "k2_c2c_tc",
-                           "c2c4096fp64": "k64_c2c", "istft": "k2_c2r + k_ola"}.get(
+                           "c2c4096fp64": "k64_c2c", "istft": "k2_c2r + k_ola",
+                           "cwt": "k2_c2r (bank rows) + k2_r2c"}.get(
                                workload, "k2_c2c")}
 
     cpu = None
@@ -539,6 +566,9 @@ def _ref_call(refimpl, workload, sample_inputs, threads):
         refimpl.c2c(sample_inputs[0], sample_inputs[1], threads=threads)
     elif workload == "stft":
         refimpl.stft(sample_inputs[0], 1024, 1024, 256, threads=threads)
+    elif workload == "cwt":
+        # the reference's own bank at this n (60 rows, as the timed bank)
+        refimpl.cwt(sample_inputs[0], threads=threads)
     elif workload == "uneven":
         # sample_inputs: (re, im, lengths) ragged; one reference batch per length
         re, im, lengths = sample_inputs
@@ -587,6 +617,8 @@ def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
         want = max(1, min(want, threads))
     elif workload == "istft":
         want = 2
+    elif workload == "cwt":
+        want = max(1, min(want, 2 * threads))
     elif workload == "uneven":
         want = 512
     sample, nbytes, sample_b = cpu_sample(workload, host_in, want)

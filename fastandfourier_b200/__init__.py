@@ -17,14 +17,14 @@ from . import _lib as C
 from ._lib import (B_CUDA, DIR_FORWARD, DIR_INVERSE, FLAG_BLUESTEIN, FLAG_MEASURE,
                    FLAG_TENSOR_CORE, PREC_FP32, PREC_FP64,
                    L_DEFAULT, L_HERMITIAN, L_INTERLEAVED, L_REAL, L_SPLIT, N_DEFAULT,
-                   N_FORWARD, N_NONE, N_ORTHO, T_FFT, T_IFFT, T_IRFFT, T_PIPELINE, T_RFFT,
-                   T_STFT)
+                   N_FORWARD, N_NONE, N_ORTHO, T_CWT, T_FFT, T_IFFT, T_IRFFT, T_PIPELINE,
+                   T_RFFT, T_STFT)
 
 __all__ = ["FafError", "Transform", "Uneven", "Server", "Request", "config", "lib", "available",
            "B_CUDA", "DIR_FORWARD", "DIR_INVERSE", "FLAG_TENSOR_CORE", "FLAG_BLUESTEIN",
            "FLAG_MEASURE", "PREC_FP32", "PREC_FP64", "L_DEFAULT", "L_HERMITIAN",
            "L_INTERLEAVED", "L_REAL", "L_SPLIT", "N_DEFAULT", "N_FORWARD", "N_NONE", "N_ORTHO",
-           "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
+           "T_CWT", "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
 
 
 class FafError(RuntimeError):
@@ -274,6 +274,25 @@ class Transform:
         return cls(C.lib().faf_cuda_create_istft(ctypes.byref(c)))
 
     @classmethod
+    def cwt(cls, n, psi):
+        """CWT filter bank (faf_cuda_create_cwt): psi holds the bank's rows,
+        (rows, >= n/2+1) real bin weights (numpy, or a torch tensor on the
+        host or the device), row 0 the lowpass when the bank has one."""
+        if hasattr(psi, "data_ptr"):
+            if str(psi.dtype) != "torch.float32" or psi.stride(-1) != 1:
+                raise FafError("cwt: psi must be float32 with contiguous rows")
+            ptr, stride = psi.data_ptr(), psi.stride(0)
+        else:
+            import numpy as np
+            psi = np.ascontiguousarray(psi, np.float32)
+            ptr, stride = psi.ctypes.data, psi.shape[-1]
+        return cls(C.lib().faf_cuda_create_cwt(n, psi.shape[0], ptr, stride))
+
+    @property
+    def cwt_rows(self):
+        return self.s.user_aux_n
+
+    @classmethod
     def chirp(cls, source):
         return cls(C.lib().chirp_compile(source.encode()))
 
@@ -412,6 +431,15 @@ class Transform:
             out = _empty_like_batch(Xr, tuple(Xr.shape[:-2]) + (L,))
         self.execute_batched(_buf(out, None, L, L_REAL), _buf(Xr, Xi, F * nb, L_HERMITIAN),
                              n_sig)
+        return out
+
+    def analyze(self, x, out=None):
+        """Forward CWT of signals x (..., n) -> W (..., rows, n)."""
+        n, rows = self.n, self.cwt_rows
+        batch = (x.numel() if hasattr(x, "numel") else x.size) // n
+        if out is None:
+            out = _empty_like_batch(x, tuple(x.shape[:-1]) + (rows, n))
+        self.execute_batched(_buf(out, None, rows * n, L_REAL), _buf(x, None, n, L_REAL), batch)
         return out
 
     def close(self):

@@ -8,6 +8,7 @@
 // not created (NULL + faf_get_error()), and every execute runs kernels.
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -563,6 +564,50 @@ extern "C" faf_transform* faf_cuda_create_istft(const faf_config* cfg) {
     DevicePlan* p = fafp::plan_istft((int)c.n, (int)c.win_length, (int)c.hop_length, err);
     if (!p) {
         fail("CUDA plan for inverse STFT n=%zu: %s", c.n, err.c_str());
+        faf_destroy_transform(t);
+        return nullptr;
+    }
+    t->device_plan = p;
+    return t;
+}
+
+// CWT filter bank: the reference builds its bank on the host at create
+// (src/faf_cwt.c:104-677) and runs x -> rows through faf_cwt_execute
+// (src/faf_cwt.c:769-847).  The device transform takes the bank's rows as
+// they are (row 0 = lowpass phi when the bank has one, then wavelets coarse
+// to fine; n/2+1 real weights per row, `psi_stride` floats apart: the
+// reference bank's n_bins_padded) and runs the execute.
+extern "C" faf_transform* faf_cuda_create_cwt(size_t n, size_t n_rows, const float* psi,
+                                              size_t psi_stride) {
+    if (n < 2 || n % 2 || !is_5_smooth(n)) {
+        fail("cwt: n=%zu must be even and 5-smooth", n);
+        return nullptr;
+    }
+    if (n_rows == 0 || !psi) {
+        fail("cwt: the bank needs at least one row (psi non-NULL)");
+        return nullptr;
+    }
+    if (psi_stride < n / 2 + 1) {
+        fail("cwt: row stride %zu is shorter than the %zu packed bins", psi_stride, n / 2 + 1);
+        return nullptr;
+    }
+    if (n_rows > (size_t)INT_MAX) {
+        fail("cwt: %zu rows", n_rows);
+        return nullptr;
+    }
+    faf_config c = faf_config_init(n);
+    c.layout = FAF_LAYOUT_REAL;
+    c.norm = FAF_NORM_NONE;
+    c.backend = FAF_BACKEND_CUDA;
+    faf_transform* t = alloc_transform();
+    if (!t) return nullptr;
+    t->type = FAF_TRANSFORM_CWT;
+    apply_resolved(t, c);
+    t->user_aux_n = n_rows;  // the reference stores the row count here too
+    std::string err;
+    DevicePlan* p = fafp::plan_cwt((int)n, (int)n_rows, psi, psi_stride, err);
+    if (!p) {
+        fail("CUDA plan for CWT n=%zu: %s", n, err.c_str());
         faf_destroy_transform(t);
         return nullptr;
     }

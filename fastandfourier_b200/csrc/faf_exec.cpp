@@ -161,6 +161,22 @@ int check_istft(const faf_transform* t, const faf_buffer* out, const faf_buffer*
     return 0;
 }
 
+// CWT (faf_cuda_create_cwt): REAL x[n] in, REAL W[rows x n] out, the
+// reference's checks (src/faf_cwt.c:769-796).
+int check_cwt(const faf_transform* t, const faf_buffer* out, const faf_buffer* in, Request& r) {
+    const size_t n = t->n, rows = t->user_aux_n;
+    if (!in->re || !out->re) return fail("cwt: buffers must provide re");
+    if (in->layout != FAF_LAYOUT_REAL || out->layout != FAF_LAYOUT_REAL)
+        return fail("cwt: layout mismatch");
+    if (in->n != n) return fail("cwt: buffer n mismatch");
+    if (in->re == out->re) return fail("cwt: in and out alias");
+    r.in_a = (const float*)in->re;
+    r.out_a = (float*)out->re;
+    r.in_len = n;
+    r.out_len = rows * n;
+    return 0;
+}
+
 int check_stft(const faf_transform* t, const faf_buffer* out, const faf_buffer* in,
                Request& r) {
     if (!in->re || !out->re) return fail("execute buffers must provide re");
@@ -511,6 +527,13 @@ int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t s
             if (!fp) return fail("STFT frame window is unavailable for this size");
         }
         break;
+    case FAF_TRANSFORM_CWT: {
+        e = fafp::exec_cwt(p, r.in_a, r.out_a, r.batch, in_dist, out_dist, st);
+        const long long nb = (long long)t->n / 2 + 1;
+        const long long cap = std::max(1LL, std::min(r.batch, (32LL << 20) / (nb * 8)));
+        launches = (int)(2 * ((r.batch + cap - 1) / cap));
+        break;
+    }
     default:
         return fail("transform type '%s' is not on the CUDA path", faf_transform_name(t->type));
     }
@@ -534,6 +557,7 @@ int build_request_typed(const faf_transform* t, faf_buffer* out, const faf_buffe
     case FAF_TRANSFORM_RFFT:
     case FAF_TRANSFORM_IRFFT: return check_rfft(t, out, in, r);
     case FAF_TRANSFORM_STFT: return check_stft(t, out, in, r);
+    case FAF_TRANSFORM_CWT: return check_cwt(t, out, in, r);
     case FAF_TRANSFORM_FFT:
     case FAF_TRANSFORM_IFFT: return check_layouts_c2c(t, out, in, r);
     default: return fail("transform type '%s' is not on the CUDA path", faf_transform_name(t->type));
@@ -654,6 +678,7 @@ extern "C" const char* faf_cuda_plan_kind(const faf_transform* t) {
     case Kind::PIPELINE: return "pipeline";
     case Kind::STFT: return "stft";
     case Kind::ISTFT: return "istft";
+    case Kind::CWT: return "cwt";
     }
     return "unknown";
 }

@@ -66,7 +66,27 @@ struct RealArgs {  // R2C / C2R / pipeline / STFT
     int nops;
     PipeOp ops[kMaxOps];
     int* err;             // bit 1 set when a bounded wait of the kernel ran out
+    // CWT rows (filtered C2R): transform b = signal * filt_rows + row reads
+    // the signal's bins weighted by filter row `row` (filt_dist floats
+    // apart) and writes output row `row` (row_len samples) of the signal
+    const float* filt;
+    long long filt_dist, row_len;
+    int filt_rows;
 };
+
+// Offsets of C2R transform b: plain, or a CWT row (RealArgs::filt).
+struct C2ROffsets {
+    long long io, oo;   // input (elements of in_dist units x fpe) / output float offsets
+    const float* f;     // filter row, or NULL
+};
+__device__ __forceinline__ C2ROffsets c2r_offsets(const RealArgs& a, long long b, int fpe) {
+    if (a.filt) {
+        const long long s = b / a.filt_rows, row = b - s * a.filt_rows;
+        return C2ROffsets{s * a.in_dist * fpe, s * a.out_dist + row * a.row_len,
+                          a.filt + row * a.filt_dist};
+    }
+    return C2ROffsets{b * a.in_dist * fpe, b * a.out_dist, nullptr};
+}
 
 struct ConvArgs {  // Rader (prime n) and Bluestein (any n)
     const float* in_re;

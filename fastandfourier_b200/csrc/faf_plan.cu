@@ -332,6 +332,7 @@ void plan_free(DevicePlan* p) {
     cudaFree(p->d_rin);
     cudaFree(p->d_rout);
     cudaFree(p->d_window);
+    cudaFree(p->d_psi);
     cudaFree(p->d_tw64);
     cudaFree(p->d_stw64);
     cudaFree(p->d_tcB);
@@ -633,6 +634,37 @@ DevicePlan* plan_istft(int n, int win, int hop, std::string& err) {
     return p;
 }
 
+// CWT filter bank (the reference's forward execute, src/faf_cwt.c:769-847):
+// the R2C of n (unscaled) and the C2R of n (1/n, the reference's NONE norm on
+// the inverse) share the inner FFT and super-twiddles; the bank's rows are
+// copied to the device, each padded to a multiple of 4 floats.  psi may be a
+// host or device pointer.
+DevicePlan* plan_cwt(int n, int rows, const float* psi, size_t psi_stride, std::string& err) {
+    if (needs_four_step(n / 2)) {
+        err = "CWT rows of " + std::to_string(n) + " samples exceed one CTA";
+        return nullptr;
+    }
+    DevicePlan* p = plan_r2c(n, false, 1.0f, err);
+    if (!p) return nullptr;
+    p->kind = Kind::CWT;
+    p->scale2 = (float)(1.0 / (double)n);
+    p->rows = rows;
+    const long long nb = n / 2 + 1;
+    p->psi_dist = (nb + 3) & ~3LL;
+    const size_t bytes = (size_t)rows * (size_t)p->psi_dist * sizeof(float);
+    cudaError_t e = cudaMalloc(&p->d_psi, bytes);
+    if (e == cudaSuccess) e = cudaMemset(p->d_psi, 0, bytes);
+    if (e == cudaSuccess)
+        e = cudaMemcpy2D(p->d_psi, (size_t)p->psi_dist * sizeof(float), psi,
+                         psi_stride * sizeof(float), (size_t)nb * sizeof(float), (size_t)rows,
+                         cudaMemcpyDefault);
+    if (!cuda_ok(e, err, "CWT bank upload")) {
+        plan_free(p);
+        return nullptr;
+    }
+    return p;
+}
+
 // ---------------------------------------------------------------------------
 // Device-pointer execution
 // ---------------------------------------------------------------------------
@@ -804,13 +836,10 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
                             p->inner.d_tw, a, st);
 }
 
-cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, long long batch,
-                     long long in_dist, long long out_dist, bool interleaved, cudaStream_t st) {
-    fafk::RealArgs a = real_args(p, batch);
-    a.in_a = Xr; a.in_b = Xi; a.out_a = y;
-    a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
+static cudaError_t launch_c2r_args(DevicePlan* p, fafk::RealArgs& a, long long batch,
+                                   cudaStream_t st) {
     if (p->large) {
-        if (a.interleaved) return cudaErrorNotSupported;
+        if (a.interleaved || a.filt) return cudaErrorNotSupported;
         return run_large(p, 2, &a, batch, st);
     }
     const int slots = p->inner.n + 1;
@@ -819,6 +848,54 @@ cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, 
                                  geometry_ct(p->inner, slots, batch), st);
     return fafk::launch_c2r(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);
+}
+
+cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, long long batch,
+                     long long in_dist, long long out_dist, bool interleaved, cudaStream_t st) {
+    fafk::RealArgs a = real_args(p, batch);
+    a.in_a = Xr; a.in_b = Xi; a.out_a = y;
+    a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
+    return launch_c2r_args(p, a, batch, st);
+}
+
+// Forward CWT of `batch` signals: per chunk of signals, the R2C into plan
+// scratch (split planes; 32 MB of spectra at most, so they stay in L2), then
+// one C2R launch over chunk x rows transforms, each reading its signal's
+// spectrum weighted by its bank row (transform order signal-major, so the
+// rows of one signal run together and re-read its spectrum from L2).
+cudaError_t exec_cwt(DevicePlan* p, const float* x, float* W, long long batch, long long in_dist,
+                     long long out_dist, cudaStream_t st) {
+    const long long nb = p->n / 2 + 1;
+    const long long cap = std::max(1LL, std::min(batch, (32LL << 20) / (nb * 8)));
+    float* spec = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(p->scratch_mu);
+        const size_t bytes = (size_t)cap * (size_t)nb * 2 * sizeof(float);
+        if (p->scratch_bytes < bytes) {
+            cudaFree(p->d_scratch);
+            p->d_scratch = nullptr;
+            p->scratch_bytes = 0;
+            cudaError_t e = cudaMalloc(&p->d_scratch, bytes);
+            if (e != cudaSuccess) return e;
+            p->scratch_bytes = bytes;
+        }
+        spec = (float*)p->d_scratch;
+    }
+    float* Xr = spec;
+    float* Xi = spec + cap * nb;
+    for (long long s0 = 0; s0 < batch; s0 += cap) {
+        const long long c = std::min(cap, batch - s0);
+        cudaError_t e = exec_r2c(p, x + s0 * in_dist, Xr, Xi, c, in_dist, nb, false, st);
+        if (e != cudaSuccess) return e;
+        fafk::RealArgs a = real_args(p, c * p->rows);
+        a.scale = p->scale2;
+        a.in_a = Xr; a.in_b = Xi; a.out_a = W + s0 * out_dist;
+        a.in_dist = nb; a.out_dist = out_dist;
+        a.filt = p->d_psi; a.filt_dist = p->psi_dist; a.filt_rows = p->rows;
+        a.row_len = p->n;
+        if ((e = launch_c2r_args(p, a, c * p->rows, st)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long batch,

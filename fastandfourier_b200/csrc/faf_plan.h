@@ -52,7 +52,8 @@ enum class Kind {
     C2R,
     PIPELINE,   // fused R2C -> ops -> C2R
     STFT,       // framed, windowed R2C
-    ISTFT       // batched C2R of frames -> windowed overlap-add
+    ISTFT,      // batched C2R of frames -> windowed overlap-add
+    CWT         // R2C of each signal, then one filtered C2R per bank row
 };
 
 struct DevicePlan {
@@ -78,6 +79,9 @@ struct DevicePlan {
     int* d_rin = nullptr;        // Rader gather
     int* d_rout = nullptr;       // Rader scatter
     float* d_window = nullptr;   // STFT window
+    float* d_psi = nullptr;      // CWT bank: rows x psi_dist real bin weights
+    int rows = 0;
+    long long psi_dist = 0;
     // FP64 plans (FAF_PREC_FP64): FP64 twiddle tables of the inner size
     bool fp64 = false;
     double2* d_tw64 = nullptr;   // W_n^i, i < inner n
@@ -111,6 +115,9 @@ DevicePlan* plan_r2c(int n, bool inverse, float scale, std::string& err);
 DevicePlan* plan_pipeline(int n, float scale_fwd, float scale_inv, std::string& err);
 DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err);
 DevicePlan* plan_istft(int n, int win, int hop, std::string& err);
+DevicePlan* plan_cwt(int n, int rows, const float* psi, size_t psi_stride, std::string& err);
+cudaError_t exec_cwt(DevicePlan* p, const float* x, float* W, long long batch, long long in_dist,
+                     long long out_dist, cudaStream_t st);
 // FP64 plans: single-CTA C2C of 5-smooth / codelet / 7-smooth lengths, and
 // R2C / C2R of even lengths whose half is such a length (up to 512 threads).
 DevicePlan* plan_c2c64(int n, bool inverse, double scale, std::string& err);

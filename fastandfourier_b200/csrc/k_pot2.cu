@@ -265,35 +265,47 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        const long long io = bi * a.in_dist * fpe;
+        const C2ROffsets o = c2r_offsets(a, bi, fpe);
+        const long long io = o.io;
         q.sync();  // the previous transform's last stage may still read ws
-        for (int k = q.t; k <= nc; k += T) {
-            cf v{0.f, 0.f};
-            if (live) {
-                if (a.interleaved) {
-                    const float2 u = __ldcs(reinterpret_cast<const float2*>(a.in_a + io) + k);
-                    v = cf{u.x, u.y};
-                } else {
-                    v = cf{__ldcs(a.in_a + io + k), __ldcs(a.in_b + io + k)};
-                }
-            }
-            mid.put(k, v);
-        }
-        q.sync();
-        for (int k = q.t; k <= nc / 2; k += T) {
-            if (k == 0) {
-                const cf x0 = mid.get(0), xn = mid.get(nc);
-                mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
+        // bin k of the input, times the bank's real weight for a CWT row
+        // (src/faf_cwt_kernels.c:22-33; the imaginary parts of DC and Nyquist,
+        // which that kernel zeroes, are never read by the pre-pass)
+        auto load = [&](int k) {
+            cf v;
+            if (a.interleaved) {
+                const float2 u = __ldcs(reinterpret_cast<const float2*>(a.in_a + io) + k);
+                v = cf{u.x, u.y};
             } else {
-                cf Zk, Znk;
-                c2r_pair(mid.get(k), mid.get(nc - k), __ldg(&a.stw[k - 1]), Zk, Znk);
-                if (k != nc - k) mid.put(k, Zk);
-                mid.put(nc - k, Znk);
+                // a CWT spectrum is re-read by every row of its signal: keep it cached
+                v = o.f ? cf{__ldg(a.in_a + io + k), __ldg(a.in_b + io + k)}
+                        : cf{__ldcs(a.in_a + io + k), __ldcs(a.in_b + io + k)};
+            }
+            if (o.f) {
+                const float w = __ldg(o.f + k);
+                v.x *= w;
+                v.y *= w;
+            }
+            return v;
+        };
+        // each thread loads whole bin pairs (k, nc - k) and runs the pre-pass
+        // on them in registers: one workspace write per bin
+        if (live) {
+            for (int k = q.t; k <= nc / 2; k += T) {
+                const cf xk = load(k), xn = load(nc - k);
+                if (k == 0) {
+                    mid.put(0, cf{xk.x + xn.x, xk.x - xn.x});
+                } else {
+                    cf Zk, Znk;
+                    c2r_pair(xk, xn, __ldg(&a.stw[k - 1]), Zk, Znk);
+                    if (k != nc - k) mid.put(k, Zk);
+                    mid.put(nc - k, Znk);
+                }
             }
         }
         q.sync();
         ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
-                          RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec}, q.sync);
+                          RealPairSink{a.out_a + o.oo, a.scale, live, vec}, q.sync);
     }
 }
 

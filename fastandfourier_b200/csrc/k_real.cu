@@ -46,7 +46,8 @@ __global__ void __launch_bounds__(1024) k_c2r(const Shape S, const float2* __res
     const long long bi = live ? b : 0;
     const int nc = S.n;
     const SmemIO mid{q.re, q.im};
-    const long long io = bi * a.in_dist * (a.interleaved ? 2 : 1);
+    const C2ROffsets o = c2r_offsets(a, bi, a.interleaved ? 2 : 1);
+    const long long io = o.io;
     for (int k = q.t; k <= nc; k += S.T) {
         cf v{0.f, 0.f};
         if (live) {
@@ -54,7 +55,13 @@ __global__ void __launch_bounds__(1024) k_c2r(const Shape S, const float2* __res
                 float2 u = __ldcs(reinterpret_cast<const float2*>(a.in_a + io) + k);
                 v = cf{u.x, u.y};
             } else {
-                v = cf{__ldcs(a.in_a + io + k), __ldcs(a.in_b + io + k)};
+                v = o.f ? cf{__ldg(a.in_a + io + k), __ldg(a.in_b + io + k)}
+                        : cf{__ldcs(a.in_a + io + k), __ldcs(a.in_b + io + k)};
+            }
+            if (o.f) {  // CWT row: the bank's real weight (src/faf_cwt_kernels.c:22-33)
+                const float w = __ldg(o.f + k);
+                v.x *= w;
+                v.y *= w;
             }
         }
         mid.put(k, v);
@@ -72,7 +79,7 @@ __global__ void __launch_bounds__(1024) k_c2r(const Shape S, const float2* __res
         }
     }
     __syncthreads();
-    RealPairSink snk{a.out_a + bi * a.out_dist, a.scale, live, vec};
+    RealPairSink snk{a.out_a + o.oo, a.scale, live, vec};
     run_fft<E>(S, q.t, q.re, q.im, tw, SmemConjSrc{q.re, q.im}, snk);
 }
 

@@ -82,6 +82,21 @@ int faf_execute_batched(const faf_transform *t, faf_buffer *out, const faf_buffe
  * (0 where that sum is below 1e-10).  Batched signals must be packed. */
 faf_transform *faf_cuda_create_istft(const faf_config *cfg);
 
+/* ---- CWT filter bank -------------------------------------------------------- */
+
+/* Replaces the execute of faf_create_cwt (include/fastandfourier.h:774;
+ * src/faf_cwt.c:769-847).  The reference builds its bank on the host at
+ * create; this transform takes the bank's rows: n_rows rows of n/2+1 real
+ * bin weights, psi_stride floats apart (host or device pointer, copied at
+ * create), row 0 = the lowpass phi when the bank has one, then the wavelets
+ * coarse to fine, as the reference bank stores them (faf_cwt_phi_f32 /
+ * faf_cwt_psi_f32).  n even and 5-smooth, n <= 32768.  faf_execute /
+ * faf_execute_batched: REAL x[n] -> REAL W[n_rows * n], row r =
+ * irfft(rfft(x) * psi_r) with 1/n on the inverse (the reference's NONE norm).
+ * The transform's user_aux_n holds n_rows, as the reference's does. */
+faf_transform *faf_cuda_create_cwt(size_t n, size_t n_rows, const float *psi,
+                                   size_t psi_stride);
+
 /* ---- uneven batches (one persistent launch) ------------------------------- */
 
 typedef struct faf_uneven faf_uneven;

@@ -155,6 +155,30 @@ def istft(Xr, Xi, n, win, hop):
     return np.where(env > 1e-10, y / np.where(env > 1e-10, env, 1.0), 0.0)
 
 
+def cwt(x, psi):
+    """Forward CWT filter bank (src/faf_cwt.c:769-847): R2C of each signal
+    once, then per bank row Y = X * psi_row with the DC and Nyquist
+    imaginary parts zeroed (src/faf_cwt_kernels.c:22-33), then the C2R with
+    the reference's NONE norm (1/n on the inverse).  x (batch, n), psi (rows,
+    n/2+1) -> W (batch, rows, n), on the oracle's own R2C / C2R."""
+    x = _f32(x)
+    psi = _f32(psi)
+    n = x.shape[-1]
+    Xr, Xi = r2c(x)
+    Yr = Xr[..., None, :] * psi
+    Yi = Xi[..., None, :] * psi
+    Yi[..., 0] = 0.0
+    Yi[..., -1] = 0.0
+    return c2r(Yr, Yi, n)
+
+
+def fp64_cwt(x, psi):
+    """The same bank in FP64 numpy."""
+    n = x.shape[-1]
+    X = np.fft.rfft(np.asarray(x, np.float64), axis=-1)
+    return np.fft.irfft(X[..., None, :] * np.asarray(psi, np.float64), n=n, axis=-1)
+
+
 def hann(n):
     w = np.empty(n, np.float32)
     lib().orc_hann(_p(w), n)

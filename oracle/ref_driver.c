@@ -36,7 +36,7 @@ static void drv_fail(const char *what) {
     snprintf(g_drv_err, sizeof(g_drv_err), "%s: %s", what, faf_get_error());
 }
 
-typedef enum { JOB_C2C, JOB_R2C, JOB_C2R, JOB_PIPE, JOB_STFT } job_kind;
+typedef enum { JOB_C2C, JOB_R2C, JOB_C2R, JOB_PIPE, JOB_STFT, JOB_CWT } job_kind;
 
 typedef struct {
     job_kind kind;
@@ -48,6 +48,7 @@ typedef struct {
     const float *h_re, *h_im;
     size_t h_bins;
     size_t win, hop, sig_len, frames; /* STFT framing */
+    size_t rows;       /* CWT: rows of the default bank (output row length n) */
     size_t b0, b1;     /* batch slice [b0, b1) */
     const float *in_re, *in_im;
     float *out_re, *out_im;
@@ -72,6 +73,11 @@ static faf_transform *make_transform(const job *j) {
     case JOB_C2R:
         c.dir = FAF_DIR_INVERSE;
         return faf_create_rfft(&c);
+    case JOB_CWT: {
+        /* The reference's default bank (Morse 20/3, L1, 10 voices, lowpass). */
+        faf_cwt_config cc = faf_cwt_config_init(j->n);
+        return faf_create_cwt(&cc);
+    }
     case JOB_PIPE: {
         faf_transform *t = chirp_compile(j->src);
         if (t && j->h_re) {
@@ -126,6 +132,11 @@ static void *run_job(void *arg) {
         case JOB_PIPE:
             in = faf_buffer_real((void *)(j->in_re + b * n), n);
             out = faf_buffer_real(j->out_re + b * n, n);
+            rc = faf_execute(t, &out, &in);
+            break;
+        case JOB_CWT:
+            in = faf_buffer_real((void *)(j->in_re + b * n), n);
+            out = faf_buffer_real(j->out_re + b * j->rows * n, j->rows * n);
             rc = faf_execute(t, &out, &in);
             break;
         case JOB_STFT: {
@@ -239,6 +250,42 @@ int refdrv_stft(size_t n, size_t win, size_t hop, size_t sig_len, size_t n_sig,
     j.frames = 1 + (sig_len - win) / hop;
     j.in_re = x; j.out_re = out_re; j.out_im = out_im;
     return run_batched(&j, n_sig * j.frames, nthreads);
+}
+
+/* The reference's default CWT bank for length n (faf_cwt_config_init +
+ * faf_create_cwt, src/faf_cwt.c:27-56,702-726): its row count, packed bin
+ * count and lowpass flag, and, when psi is non-NULL, its rows in execute
+ * order (row 0 = lowpass phi if present, then wavelets coarse -> fine), each
+ * n/2+1 floats, copied from faf_cwt_phi_f32 / faf_cwt_psi_f32. */
+int refdrv_cwt_bank(size_t n, size_t *n_rows, size_t *n_bins, int *has_lowpass, float *psi) {
+    faf_cwt_config cc = faf_cwt_config_init(n);
+    faf_transform *t = faf_create_cwt(&cc);
+    if (!t) { drv_fail("cwt create"); return -1; }
+    const size_t rows = faf_cwt_n_rows(t), nb = faf_cwt_n_bins(t);
+    const int lp = faf_cwt_has_lowpass(t);
+    if (n_rows) *n_rows = rows;
+    if (n_bins) *n_bins = nb;
+    if (has_lowpass) *has_lowpass = lp;
+    if (psi) {
+        size_t r = 0;
+        if (lp) memcpy(psi + (r++) * nb, faf_cwt_phi_f32(t), nb * sizeof(float));
+        for (size_t j = 0; j < faf_cwt_n_scales(t); j++)
+            memcpy(psi + (r++) * nb, faf_cwt_psi_f32(t, j), nb * sizeof(float));
+    }
+    faf_destroy_transform(t);
+    return 0;
+}
+
+/* Forward CWT of `batch` signals with the default bank; W is
+ * [batch][rows][n] (src/faf_cwt.c:769-847 per signal). */
+int refdrv_cwt(size_t n, size_t batch, const float *x, float *W, int nthreads) {
+    size_t rows = 0;
+    if (refdrv_cwt_bank(n, &rows, NULL, NULL, NULL) != 0) return -1;
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_CWT; j.n = n; j.rows = rows;
+    j.in_re = x; j.out_re = W;
+    return run_batched(&j, batch, nthreads);
 }
 
 /* Reference size policy, exposed for the parity tests of the planner. */

@@ -74,6 +74,9 @@ def lib():
         L.refdrv_pipeline.argtypes = [ctypes.c_char_p, sz, _f32p, _f32p, sz, sz,
                                       _f32p, _f32p, i]
         L.refdrv_stft.argtypes = [sz, sz, sz, sz, sz, _f32p, _f32p, _f32p, i]
+        szp = ctypes.POINTER(sz)
+        L.refdrv_cwt_bank.argtypes = [sz, szp, szp, ctypes.POINTER(i), _f32p]
+        L.refdrv_cwt.argtypes = [sz, sz, _f32p, _f32p, i]
         L.refdrv_is_size_supported.argtypes = [i, sz]
         L.refdrv_recommended_size.argtypes = [i, sz]
         L.refdrv_recommended_size.restype = sz
@@ -156,6 +159,27 @@ def stft(x, n, win, hop, threads=1):
     Xr, Xi = np.empty(shp, np.float32), np.empty(shp, np.float32)
     _check(lib().refdrv_stft(n, win, hop, L, n_sig, _p(x), _p(Xr), _p(Xi), threads))
     return Xr, Xi
+
+
+def cwt_bank(n):
+    """The reference's default CWT bank for length n: (psi rows in execute
+    order, (rows, n/2+1) float32; has_lowpass)."""
+    rows, nb, lp = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_int()
+    _check(lib().refdrv_cwt_bank(n, ctypes.byref(rows), ctypes.byref(nb), ctypes.byref(lp), None))
+    psi = np.empty((rows.value, nb.value), np.float32)
+    _check(lib().refdrv_cwt_bank(n, None, None, None, _p(psi)))
+    return psi, bool(lp.value)
+
+
+def cwt(x, threads=1):
+    """The reference's forward CWT (default bank) of signals x (batch, n):
+    W (batch, rows, n)."""
+    x = _f32(x)
+    n = x.shape[-1]
+    rows = cwt_bank(n)[0].shape[0]
+    W = np.empty(x.shape[:-1] + (rows, n), np.float32)
+    _check(lib().refdrv_cwt(n, x.size // n, _p(x), _p(W), threads))
+    return W
 
 
 def is_size_supported(ttype, n):

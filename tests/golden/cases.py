@@ -12,6 +12,7 @@ BLUESTEIN = [23, 47, 307]
 BIG_C2C = [16384]
 REAL_SIZES = [2, 16, 64, 4096, 6000]
 STFT = (1024, 1024, 256, 4096)  # n, win, hop, signal length
+CWT = [512, 1000]  # signal lengths; the reference's default bank (Morse 20/3, 10 voices, lowpass)
 FLAG_BLUESTEIN = 1 << 12
 
 

@@ -118,6 +118,10 @@ def main():
     xs = cases.real_input(L, batch=2, seed=4)
     Xr, Xi = refimpl.stft(xs, n, win, hop)
     out["stft"] = np.stack([Xr, Xi])
+    for n in cases.CWT:
+        psi, _ = refimpl.cwt_bank(n)
+        out[f"cwt_psi_{n}"] = psi
+        out[f"cwt_{n}"] = refimpl.cwt(cases.real_input(n, batch=1, seed=9))
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
 
     policy = {"supported": {}, "recommended": {}, "create": []}

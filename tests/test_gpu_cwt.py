@@ -1,0 +1,116 @@
+"""CWT filter bank (faf_cuda_create_cwt): the device execute of the
+reference's forward CWT (src/faf_cwt.c:769-847) against the reference's own
+outputs for its default banks (golden fixtures), the oracle, and FP64 numpy,
+over power-of-two and 5-smooth lengths, batches, host and device buffers, and
+the create-time checks."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import REL_L2_TOL, ROOT, seeded
+from oracle import orc
+
+pytestmark = pytest.mark.gpu
+
+GOLD = os.path.join(ROOT, "tests", "golden")
+sys.path.insert(0, GOLD)
+import cases  # noqa: E402
+
+
+def rel(got, want):
+    return float(np.linalg.norm(got - want) / np.linalg.norm(want))
+
+
+def bank(rows, n, seed):
+    """Seeded smooth bandpass rows (positive, like analytic wavelet banks)."""
+    nb = n // 2 + 1
+    k = np.arange(nb)[None, :]
+    c = np.geomspace(2.0, nb * 0.8, rows)[:, None]
+    rng = seeded(seed)
+    return (np.exp(-0.5 * ((k - c) / (0.25 * c + 1.0)) ** 2) * rng.uniform(0.5, 2, (rows, 1))).astype(np.float32)
+
+
+@pytest.mark.parametrize("n", cases.CWT)
+def test_cwt_matches_reference_golden(cuda, n):
+    import fastandfourier_b200 as F
+    torch = cuda
+    g = np.load(os.path.join(GOLD, "golden.npz"))
+    psi, want = g[f"cwt_psi_{n}"], g[f"cwt_{n}"]
+    x = cases.real_input(n, batch=1, seed=9)
+    t = F.Transform.cwt(n, psi)
+    assert t.type == F.T_CWT and t.kind == "cwt" and t.cwt_rows == psi.shape[0]
+    W = t.analyze(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert W.shape == want.shape
+    assert rel(W, want) <= REL_L2_TOL
+    assert rel(W, orc.fp64_cwt(x, psi)) <= REL_L2_TOL
+    assert t.wait_status() == 0
+
+
+@pytest.mark.parametrize("n", [16, 256, 1000, 4096, 6000, 32768])
+def test_cwt_batches_match_oracle(cuda, n):
+    import fastandfourier_b200 as F
+    torch = cuda
+    psi = bank(7, n, n)
+    x = seeded(n + 1).standard_normal((3, n)).astype(np.float32)
+    t = F.Transform.cwt(n, psi)
+    W = t.analyze(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert W.shape == (3, 7, n)
+    assert rel(W, orc.cwt(x, psi)) <= REL_L2_TOL
+    assert rel(W, orc.fp64_cwt(x, psi)) <= REL_L2_TOL
+
+
+def test_cwt_host_buffers_and_device_bank(cuda):
+    import fastandfourier_b200 as F
+    torch = cuda
+    n = 2048
+    psi = bank(5, n, 3)
+    x = seeded(5).standard_normal((4, n)).astype(np.float32)
+    want = orc.fp64_cwt(x, psi)
+    t_host = F.Transform.cwt(n, psi)                       # bank from host memory
+    assert rel(t_host.analyze(x), want) <= REL_L2_TOL      # host signal and output
+    t_dev = F.Transform.cwt(n, torch.from_numpy(psi).cuda())  # bank from device memory
+    assert rel(t_dev.analyze(torch.from_numpy(x).cuda()).cpu().numpy(), want) <= REL_L2_TOL
+
+
+def test_cwt_padded_bank_rows(cuda):
+    """Rows `psi_stride` floats apart, as the reference bank pads them."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n = 1000
+    psi = bank(4, n, 8)
+    padded = np.zeros((4, 512), np.float32)
+    padded[:, :501] = psi
+    padded[:, 501:] = 1e9  # the padding must never be read
+    x = seeded(9).standard_normal((2, n)).astype(np.float32)
+    W = F.Transform.cwt(n, padded).analyze(torch.from_numpy(x).cuda()).cpu().numpy()
+    assert rel(W, orc.fp64_cwt(x, psi)) <= REL_L2_TOL
+
+
+def test_cwt_large_batch_chunks(cuda):
+    """More signals than one 32 MB chunk of spectra: two R2C / C2R rounds."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n, rows, batch = 4096, 3, 2050
+    psi = bank(rows, n, 11)
+    x = seeded(12).standard_normal((batch, n)).astype(np.float32)
+    t = F.Transform.cwt(n, psi)
+    W = t.analyze(torch.from_numpy(x).cuda())
+    assert F.lib().faf_cuda_last_launches() == 4
+    pick = [0, 1, 2046, 2047, 2048, 2049]
+    got = W[pick].cpu().numpy()
+    assert rel(got, orc.fp64_cwt(x[pick], psi)) <= REL_L2_TOL
+
+
+def test_cwt_create_errors(cuda):
+    import fastandfourier_b200 as F
+    psi = np.ones((2, 40000), np.float32)
+    with pytest.raises(F.FafError, match="exceed one CTA"):
+        F.Transform.cwt(65536, np.ones((2, 32769), np.float32))
+    with pytest.raises(F.FafError, match="even and 5-smooth"):
+        F.Transform.cwt(14, psi)
+    t = F.Transform.cwt(64, psi[:, :33])
+    with pytest.raises(F.FafError, match="buffer n mismatch"):
+        t.execute(F._buf(np.zeros(2 * 64, np.float32), None, 2 * 64, F.L_REAL),
+                  F._buf(np.zeros(32, np.float32), None, 32, F.L_REAL))

@@ -218,3 +218,20 @@ def test_stream_handles():
     assert F._stream_handle(S(0)) == F.CUDA_STREAM_LEGACY == 1
     assert F._stream_handle(S(0x7f00deadbe00)) == 0x7f00deadbe00
     assert F._stream_handle(0x5000) == 0x5000
+
+
+def test_cwt_create_checks():
+    """faf_cuda_create_cwt validates n, the bank and its stride before any
+    device work, with the reference's wording where it has one."""
+    import numpy as np
+    import fastandfourier_b200 as F
+    L = F.lib()
+    psi = np.ones((2, 64), np.float32)
+    p = psi.ctypes.data
+    for n, rows, ptr, stride, msg in [(15, 2, p, 64, "even and 5-smooth"),
+                                     (14, 2, p, 64, "even and 5-smooth"),
+                                     (64, 0, p, 64, "at least one row"),
+                                     (64, 2, None, 64, "at least one row"),
+                                     (120, 2, p, 60, "shorter than the 61 packed bins")]:
+        assert not L.faf_cuda_create_cwt(n, rows, ptr, stride)
+        assert msg in F.C.error()

@@ -168,3 +168,14 @@ def test_reference_fp64_c2c_vs_numpy(n):
         want = np.fft.ifft(z, axis=-1) if inv else np.fft.fft(z, axis=-1)
         got = yr + 1j * yi
         assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 1e-12
+
+
+@pytest.mark.parametrize("n", cases.CWT)
+def test_oracle_cwt_vs_reference(gold, n):
+    """The oracle's CWT (its own R2C, bank multiply, C2R) against the
+    reference's faf_cwt_execute on the reference's default bank."""
+    x = cases.real_input(n, batch=1, seed=9)
+    psi, want = gold[f"cwt_psi_{n}"], gold[f"cwt_{n}"]
+    got = orc.cwt(x, psi)
+    assert orc.rel_l2(got, want) <= TOL
+    assert orc.rel_l2(got, orc.fp64_cwt(x, psi)) <= TOL
