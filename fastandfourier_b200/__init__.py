@@ -17,14 +17,14 @@ from . import _lib as C
 from ._lib import (B_CUDA, DIR_FORWARD, DIR_INVERSE, FLAG_BLUESTEIN, FLAG_MEASURE,
                    FLAG_TENSOR_CORE, PREC_FP32, PREC_FP64,
                    L_DEFAULT, L_HERMITIAN, L_INTERLEAVED, L_REAL, L_SPLIT, N_DEFAULT,
-                   N_FORWARD, N_NONE, N_ORTHO, T_CWT, T_FFT, T_IFFT, T_IRFFT, T_PIPELINE,
-                   T_RFFT, T_STFT)
+                   N_FORWARD, N_NONE, N_ORTHO, T_CWT, T_FFT, T_ICWT, T_IFFT, T_IRFFT,
+                   T_PIPELINE, T_RFFT, T_STFT)
 
 __all__ = ["FafError", "Transform", "Uneven", "Server", "Request", "config", "lib", "available",
            "B_CUDA", "DIR_FORWARD", "DIR_INVERSE", "FLAG_TENSOR_CORE", "FLAG_BLUESTEIN",
            "FLAG_MEASURE", "PREC_FP32", "PREC_FP64", "L_DEFAULT", "L_HERMITIAN",
            "L_INTERLEAVED", "L_REAL", "L_SPLIT", "N_DEFAULT", "N_FORWARD", "N_NONE", "N_ORTHO",
-           "T_CWT", "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
+           "T_CWT", "T_ICWT", "T_FFT", "T_IFFT", "T_IRFFT", "T_PIPELINE", "T_RFFT", "T_STFT"]
 
 
 class FafError(RuntimeError):
@@ -288,6 +288,33 @@ class Transform:
             ptr, stride = psi.ctypes.data, psi.shape[-1]
         return cls(C.lib().faf_cuda_create_cwt(n, psi.shape[0], ptr, stride))
 
+    @classmethod
+    def icwt_dual(cls, n, dual):
+        """Dual-frame inverse CWT (faf_cuda_create_icwt_dual): dual rows
+        (rows, >= n/2+1), numpy or torch."""
+        if hasattr(dual, "data_ptr"):
+            ptr, stride = dual.data_ptr(), dual.stride(0)
+        else:
+            import numpy as np
+            dual = np.ascontiguousarray(dual, np.float32)
+            ptr, stride = dual.ctypes.data, dual.shape[-1]
+        return cls(C.lib().faf_cuda_create_icwt_dual(n, dual.shape[0], ptr, stride))
+
+    @classmethod
+    def icwt_l1(cls, n, rows, has_lowpass, dlog, c):
+        """L1 one-integral inverse CWT (faf_cuda_create_icwt_l1)."""
+        return cls(C.lib().faf_cuda_create_icwt_l1(n, rows, int(has_lowpass), dlog, c))
+
+    @staticmethod
+    def cwt_dual_rows(psi, eps=1e-6):
+        """The dual-frame rows of a bank as the reference derives them
+        (src/faf_cwt.c:440-482): psi_r / (sum_r psi_r^2 + eps), the sum over
+        rows in FP64, zero where that sum is 0."""
+        import numpy as np
+        p = np.asarray(psi, np.float64)
+        s = np.sum(p * p, axis=0)
+        return np.where(s > 0, p / (s + eps), 0.0).astype(np.float32)
+
     @property
     def cwt_rows(self):
         return self.s.user_aux_n
@@ -431,6 +458,15 @@ class Transform:
             out = _empty_like_batch(Xr, tuple(Xr.shape[:-2]) + (L,))
         self.execute_batched(_buf(out, None, L, L_REAL), _buf(Xr, Xi, F * nb, L_HERMITIAN),
                              n_sig)
+        return out
+
+    def synthesize(self, W, out=None):
+        """Inverse CWT of coefficients W (..., rows, n) -> x (..., n)."""
+        n, rows = self.n, self.cwt_rows
+        batch = (W.numel() if hasattr(W, "numel") else W.size) // (rows * n)
+        if out is None:
+            out = _empty_like_batch(W, tuple(W.shape[:-2]) + (n,))
+        self.execute_batched(_buf(out, None, n, L_REAL), _buf(W, None, rows * n, L_REAL), batch)
         return out
 
     def analyze(self, x, out=None):

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(_HERE, "libfaf_b200.so")
 # enum values (include/fastandfourier.h)
 PREC_FP16, PREC_FP32, PREC_FP64 = 1, 3, 4
 (T_FFT, T_IFFT, T_RFFT, T_IRFFT) = (0, 1, 2, 3)
-T_STFT, T_PIPELINE, T_CWT = 12, 20, 21
+T_STFT, T_PIPELINE, T_CWT, T_ICWT = 12, 20, 21, 22
 L_DEFAULT, L_SPLIT, L_HERMITIAN, L_REAL, L_INTERLEAVED = 0, 1, 2, 3, 4
 N_DEFAULT, N_NONE, N_ORTHO, N_FORWARD, N_LAZY, N_JPEG2000 = 0, 1, 2, 3, 4, 5
 DIR_FORWARD, DIR_INVERSE = 0, 1
@@ -134,6 +134,10 @@ _SIGS = [
     ("faf_cuda_get_stream", ctypes.c_void_p, [TP]),
     ("faf_cuda_wait_status", ctypes.c_int, [TP]),
     ("faf_cuda_create_cwt", TP, [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]),
+    ("faf_cuda_create_icwt_dual", TP,
+     [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]),
+    ("faf_cuda_create_icwt_l1", TP,
+     [ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int, ctypes.c_double, ctypes.c_double]),
     ("faf_cuda_synchronize", ctypes.c_int, [TP]),
     ("faf_cuda_execute_c2c_noalloc", ctypes.c_int,
      [TP] + [ctypes.c_void_p] * 4 + [ctypes.c_size_t]),

@@ -615,6 +615,73 @@ extern "C" faf_transform* faf_cuda_create_cwt(size_t n, size_t n_rows, const flo
     return t;
 }
 
+// Shared checks and the transform object of the two inverse CWT forms.
+static faf_transform* icwt_transform(size_t n, size_t n_rows) {
+    if (n < 2 || n % 2 || !is_5_smooth(n)) {
+        fail("cwt: n=%zu must be even and 5-smooth", n);
+        return nullptr;
+    }
+    if (n_rows == 0 || n_rows > (size_t)INT_MAX) {
+        fail("cwt: the bank needs at least one row");
+        return nullptr;
+    }
+    faf_config c = faf_config_init(n);
+    c.layout = FAF_LAYOUT_REAL;
+    c.norm = FAF_NORM_NONE;
+    c.dir = FAF_DIR_INVERSE;
+    c.backend = FAF_BACKEND_CUDA;
+    faf_transform* t = alloc_transform();
+    if (!t) return nullptr;
+    t->type = FAF_TRANSFORM_ICWT;
+    apply_resolved(t, c);
+    t->user_aux_n = n_rows;
+    return t;
+}
+
+// Dual-frame inverse CWT (faf_create_icwt with FAF_CWT_INV_DUAL,
+// src/faf_cwt.c:728-762 and 935-985): the bank's dual rows, as the reference
+// derives them from its analysis rows (src/faf_cwt.c:440-482).
+extern "C" faf_transform* faf_cuda_create_icwt_dual(size_t n, size_t n_rows, const float* dual,
+                                                    size_t dual_stride) {
+    if (!dual || dual_stride < n / 2 + 1) {
+        fail("cwt: dual rows missing or stride %zu shorter than the %zu packed bins", dual_stride,
+             n / 2 + 1);
+        return nullptr;
+    }
+    faf_transform* t = icwt_transform(n, n_rows);
+    if (!t) return nullptr;
+    std::string err;
+    DevicePlan* p = fafp::plan_icwt_dual((int)n, (int)n_rows, dual, dual_stride, err);
+    if (!p) {
+        fail("CUDA plan for inverse CWT n=%zu: %s", n, err.c_str());
+        faf_destroy_transform(t);
+        return nullptr;
+    }
+    t->device_plan = p;
+    return t;
+}
+
+// L1 one-integral inverse CWT (FAF_CWT_INV_L1, src/faf_cwt.c:879-930):
+// dlog = ln 2 / voices, C = the bank report's admissibility_C (<= 0 means 1).
+extern "C" faf_transform* faf_cuda_create_icwt_l1(size_t n, size_t n_rows, int has_lowpass,
+                                                  double dlog, double C) {
+    if (has_lowpass && n_rows < 2) {
+        fail("cwt: a bank with a lowpass row needs at least one wavelet row");
+        return nullptr;
+    }
+    faf_transform* t = icwt_transform(n, n_rows);
+    if (!t) return nullptr;
+    std::string err;
+    DevicePlan* p = fafp::plan_icwt_l1((int)n, (int)n_rows, has_lowpass, dlog, C, err);
+    if (!p) {
+        fail("CUDA plan for inverse CWT n=%zu: %s", n, err.c_str());
+        faf_destroy_transform(t);
+        return nullptr;
+    }
+    t->device_plan = p;
+    return t;
+}
+
 extern "C" faf_transform* faf_create_inverse(const faf_transform* fwd) {
     if (!fwd) {
         fail("faf_create_inverse: transform is NULL");

@@ -177,6 +177,20 @@ int check_cwt(const faf_transform* t, const faf_buffer* out, const faf_buffer* i
     return 0;
 }
 
+// Inverse CWT: REAL W[rows x n] in, REAL x[n] out (src/faf_cwt.c:849-877).
+int check_icwt(const faf_transform* t, const faf_buffer* out, const faf_buffer* in, Request& r) {
+    const size_t n = t->n, rows = t->user_aux_n;
+    if (!in->re || !out->re) return fail("cwt: buffers must provide re");
+    if (in->layout != FAF_LAYOUT_REAL || out->layout != FAF_LAYOUT_REAL)
+        return fail("cwt: layout mismatch");
+    if (out->n != n) return fail("cwt: buffer n mismatch");
+    r.in_a = (const float*)in->re;
+    r.out_a = (float*)out->re;
+    r.in_len = rows * n;
+    r.out_len = n;
+    return 0;
+}
+
 int check_stft(const faf_transform* t, const faf_buffer* out, const faf_buffer* in,
                Request& r) {
     if (!in->re || !out->re) return fail("execute buffers must provide re");
@@ -534,6 +548,20 @@ int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t s
         launches = (int)(2 * ((r.batch + cap - 1) / cap));
         break;
     }
+    case FAF_TRANSFORM_ICWT: {
+        if (r.batch > 1 && in_dist != (long long)r.in_len)
+            return fail("batched inverse CWT coefficients must be packed (rows x n per signal)");
+        e = fafp::exec_icwt(p, r.in_a, r.out_a, r.batch, in_dist, out_dist, st);
+        if (p->kind == Kind::ICWT_L1) {
+            launches = 1;
+        } else {
+            const long long yd = p->psi_dist;
+            const long long cap =
+                std::max(1LL, std::min(r.batch, (64LL << 20) / ((long long)p->rows * yd * 8)));
+            launches = (int)(3 * ((r.batch + cap - 1) / cap));
+        }
+        break;
+    }
     default:
         return fail("transform type '%s' is not on the CUDA path", faf_transform_name(t->type));
     }
@@ -558,6 +586,7 @@ int build_request_typed(const faf_transform* t, faf_buffer* out, const faf_buffe
     case FAF_TRANSFORM_IRFFT: return check_rfft(t, out, in, r);
     case FAF_TRANSFORM_STFT: return check_stft(t, out, in, r);
     case FAF_TRANSFORM_CWT: return check_cwt(t, out, in, r);
+    case FAF_TRANSFORM_ICWT: return check_icwt(t, out, in, r);
     case FAF_TRANSFORM_FFT:
     case FAF_TRANSFORM_IFFT: return check_layouts_c2c(t, out, in, r);
     default: return fail("transform type '%s' is not on the CUDA path", faf_transform_name(t->type));
@@ -679,6 +708,8 @@ extern "C" const char* faf_cuda_plan_kind(const faf_transform* t) {
     case Kind::STFT: return "stft";
     case Kind::ISTFT: return "istft";
     case Kind::CWT: return "cwt";
+    case Kind::ICWT_DUAL: return "icwt-dual";
+    case Kind::ICWT_L1: return "icwt-l1";
     }
     return "unknown";
 }

@@ -191,6 +191,12 @@ struct Real64Args {
     double scale;
     const double2* stw;    // super-twiddles, FP64
 };
+cudaError_t launch_icwt_acc(const float* yr, const float* yi, const float* dual, long long nb,
+                            long long ydist, long long ddist, int rows, long long batch,
+                            float* ar, float* ai, cudaStream_t st);
+cudaError_t launch_icwt_l1(const float* W, long long n, long long in_dist, int rows, int lowpass,
+                           float dlog, float C, long long batch, float* x, long long out_dist,
+                           cudaStream_t st);
 cudaError_t launch_fp64(int kind, const fafd::Shape& S, const Geometry& g, const double2* tw,
                         const void* args, cudaStream_t st);
 

@@ -634,6 +634,9 @@ DevicePlan* plan_istft(int n, int win, int hop, std::string& err) {
     return p;
 }
 
+static bool upload_rows(DevicePlan* p, int rows, const float* src, size_t stride,
+                        std::string& err);
+
 // CWT filter bank (the reference's forward execute, src/faf_cwt.c:769-847):
 // the R2C of n (unscaled) and the C2R of n (1/n, the reference's NONE norm on
 // the inverse) share the inner FFT and super-twiddles; the bank's rows are
@@ -648,20 +651,56 @@ DevicePlan* plan_cwt(int n, int rows, const float* psi, size_t psi_stride, std::
     if (!p) return nullptr;
     p->kind = Kind::CWT;
     p->scale2 = (float)(1.0 / (double)n);
+    if (!upload_rows(p, rows, psi, psi_stride, err)) {
+        plan_free(p);
+        return nullptr;
+    }
+    return p;
+}
+
+// Bank rows to the device, each padded to a multiple of 4 floats.
+static bool upload_rows(DevicePlan* p, int rows, const float* src, size_t stride,
+                        std::string& err) {
+    const long long nb = p->n / 2 + 1;
     p->rows = rows;
-    const long long nb = n / 2 + 1;
     p->psi_dist = (nb + 3) & ~3LL;
     const size_t bytes = (size_t)rows * (size_t)p->psi_dist * sizeof(float);
     cudaError_t e = cudaMalloc(&p->d_psi, bytes);
     if (e == cudaSuccess) e = cudaMemset(p->d_psi, 0, bytes);
     if (e == cudaSuccess)
-        e = cudaMemcpy2D(p->d_psi, (size_t)p->psi_dist * sizeof(float), psi,
-                         psi_stride * sizeof(float), (size_t)nb * sizeof(float), (size_t)rows,
+        e = cudaMemcpy2D(p->d_psi, (size_t)p->psi_dist * sizeof(float), src,
+                         stride * sizeof(float), (size_t)nb * sizeof(float), (size_t)rows,
                          cudaMemcpyDefault);
-    if (!cuda_ok(e, err, "CWT bank upload")) {
+    return cuda_ok(e, err, "CWT bank upload");
+}
+
+// Dual-frame inverse CWT (src/faf_cwt.c:935-985): the R2C of n (unscaled)
+// and the C2R of n (1/n) with the bank's dual rows.
+DevicePlan* plan_icwt_dual(int n, int rows, const float* dual, size_t stride, std::string& err) {
+    if (needs_four_step(n / 2)) {
+        err = "CWT rows of " + std::to_string(n) + " samples exceed one CTA";
+        return nullptr;
+    }
+    DevicePlan* p = plan_r2c(n, false, 1.0f, err);
+    if (!p) return nullptr;
+    p->kind = Kind::ICWT_DUAL;
+    p->scale2 = (float)(1.0 / (double)n);
+    if (!upload_rows(p, rows, dual, stride, err)) {
         plan_free(p);
         return nullptr;
     }
+    return p;
+}
+
+// L1 one-integral inverse CWT (src/faf_cwt.c:879-930): no FFT, only the
+// weighted row sum.
+DevicePlan* plan_icwt_l1(int n, int rows, int lowpass, double dlog, double c, std::string& err) {
+    (void)err;
+    DevicePlan* p = new_plan(Kind::ICWT_L1, n);
+    p->rows = rows;
+    p->lowpass = lowpass ? 1 : 0;
+    p->dlog = dlog;
+    p->cwt_c = c > 0.0 ? c : 1.0;  // the reference takes C <= 0 as 1
     return p;
 }
 
@@ -858,6 +897,58 @@ cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, 
     return launch_c2r_args(p, a, batch, st);
 }
 
+// Plan scratch of at least `bytes` (scratch_mu; the host-buffer path holds mu).
+static cudaError_t plan_scratch(DevicePlan* p, size_t bytes, float** out) {
+    std::lock_guard<std::mutex> lk(p->scratch_mu);
+    if (p->scratch_bytes < bytes) {
+        cudaFree(p->d_scratch);
+        p->d_scratch = nullptr;
+        p->scratch_bytes = 0;
+        cudaError_t e = cudaMalloc(&p->d_scratch, bytes);
+        if (e != cudaSuccess) return e;
+        p->scratch_bytes = bytes;
+    }
+    *out = (float*)p->d_scratch;
+    return cudaSuccess;
+}
+
+// Inverse CWT of `batch` coefficient sets W[rows x n] (packed when batch >
+// 1: in_dist = rows * n).  Dual frame: per chunk of signals (64 MB of row
+// spectra at most, so they stay in L2), the R2C of every row, the
+// dual-weighted sum over rows per bin, and the C2R of the sums.  L1: one
+// pass of weighted row sums.
+cudaError_t exec_icwt(DevicePlan* p, const float* W, float* x, long long batch, long long in_dist,
+                      long long out_dist, cudaStream_t st) {
+    const long long n = p->n, rows = p->rows;
+    if (p->kind == Kind::ICWT_L1)
+        return fafk::launch_icwt_l1(W, n, in_dist, (int)rows, p->lowpass, (float)p->dlog,
+                                    (float)p->cwt_c, batch, x, out_dist, st);
+    const long long nb = n / 2 + 1, yd = p->psi_dist;
+    const long long cap = std::max(1LL, std::min(batch, (64LL << 20) / (rows * yd * 8)));
+    float* sc = nullptr;
+    cudaError_t e = plan_scratch(p, (size_t)(cap * rows * yd + cap * nb) * 2 * sizeof(float), &sc);
+    if (e != cudaSuccess) return e;
+    float* Yr = sc;
+    float* Yi = Yr + cap * rows * yd;
+    float* Ar = Yi + cap * rows * yd;
+    float* Ai = Ar + cap * nb;
+    for (long long s0 = 0; s0 < batch; s0 += cap) {
+        const long long c = std::min(cap, batch - s0);
+        if ((e = exec_r2c(p, W + s0 * in_dist, Yr, Yi, c * rows, n, yd, false, st)) !=
+            cudaSuccess)
+            return e;
+        if ((e = fafk::launch_icwt_acc(Yr, Yi, p->d_psi, nb, yd, p->psi_dist, (int)rows, c, Ar,
+                                       Ai, st)) != cudaSuccess)
+            return e;
+        fafk::RealArgs a = real_args(p, c);
+        a.scale = p->scale2;
+        a.in_a = Ar; a.in_b = Ai; a.out_a = x + s0 * out_dist;
+        a.in_dist = nb; a.out_dist = out_dist;
+        if ((e = launch_c2r_args(p, a, c, st)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // Forward CWT of `batch` signals: per chunk of signals, the R2C into plan
 // scratch (split planes; 32 MB of spectra at most, so they stay in L2), then
 // one C2R launch over chunk x rows transforms, each reading its signal's
@@ -868,19 +959,8 @@ cudaError_t exec_cwt(DevicePlan* p, const float* x, float* W, long long batch, l
     const long long nb = p->n / 2 + 1;
     const long long cap = std::max(1LL, std::min(batch, (32LL << 20) / (nb * 8)));
     float* spec = nullptr;
-    {
-        std::lock_guard<std::mutex> lk(p->scratch_mu);
-        const size_t bytes = (size_t)cap * (size_t)nb * 2 * sizeof(float);
-        if (p->scratch_bytes < bytes) {
-            cudaFree(p->d_scratch);
-            p->d_scratch = nullptr;
-            p->scratch_bytes = 0;
-            cudaError_t e = cudaMalloc(&p->d_scratch, bytes);
-            if (e != cudaSuccess) return e;
-            p->scratch_bytes = bytes;
-        }
-        spec = (float*)p->d_scratch;
-    }
+    cudaError_t e0 = plan_scratch(p, (size_t)cap * (size_t)nb * 2 * sizeof(float), &spec);
+    if (e0 != cudaSuccess) return e0;
     float* Xr = spec;
     float* Xi = spec + cap * nb;
     for (long long s0 = 0; s0 < batch; s0 += cap) {

@@ -53,7 +53,9 @@ enum class Kind {
     PIPELINE,   // fused R2C -> ops -> C2R
     STFT,       // framed, windowed R2C
     ISTFT,      // batched C2R of frames -> windowed overlap-add
-    CWT         // R2C of each signal, then one filtered C2R per bank row
+    CWT,        // R2C of each signal, then one filtered C2R per bank row
+    ICWT_DUAL,  // R2C of every row, dual-weighted sum over rows, C2R
+    ICWT_L1     // weighted sum of the time-domain rows
 };
 
 struct DevicePlan {
@@ -79,9 +81,11 @@ struct DevicePlan {
     int* d_rin = nullptr;        // Rader gather
     int* d_rout = nullptr;       // Rader scatter
     float* d_window = nullptr;   // STFT window
-    float* d_psi = nullptr;      // CWT bank: rows x psi_dist real bin weights
+    float* d_psi = nullptr;      // CWT bank (dual rows for ICWT_DUAL): rows x psi_dist weights
     int rows = 0;
     long long psi_dist = 0;
+    int lowpass = 0;             // ICWT_L1: row 0 is the lowpass
+    double dlog = 0.0, cwt_c = 1.0;  // ICWT_L1: log-scale step and admissibility constant
     // FP64 plans (FAF_PREC_FP64): FP64 twiddle tables of the inner size
     bool fp64 = false;
     double2* d_tw64 = nullptr;   // W_n^i, i < inner n
@@ -116,6 +120,10 @@ DevicePlan* plan_pipeline(int n, float scale_fwd, float scale_inv, std::string& 
 DevicePlan* plan_stft(int n, int win, int hop, float scale, std::string& err);
 DevicePlan* plan_istft(int n, int win, int hop, std::string& err);
 DevicePlan* plan_cwt(int n, int rows, const float* psi, size_t psi_stride, std::string& err);
+DevicePlan* plan_icwt_dual(int n, int rows, const float* dual, size_t stride, std::string& err);
+DevicePlan* plan_icwt_l1(int n, int rows, int lowpass, double dlog, double c, std::string& err);
+cudaError_t exec_icwt(DevicePlan* p, const float* W, float* x, long long batch, long long in_dist,
+                      long long out_dist, cudaStream_t st);
 cudaError_t exec_cwt(DevicePlan* p, const float* x, float* W, long long batch, long long in_dist,
                      long long out_dist, cudaStream_t st);
 // FP64 plans: single-CTA C2C of 5-smooth / codelet / 7-smooth lengths, and

@@ -97,6 +97,21 @@ faf_transform *faf_cuda_create_istft(const faf_config *cfg);
 faf_transform *faf_cuda_create_cwt(size_t n, size_t n_rows, const float *psi,
                                    size_t psi_stride);
 
+/* Replace the execute of faf_create_icwt (include/fastandfourier.h:783;
+ * src/faf_cwt.c:849-985).  faf_execute / faf_execute_batched: REAL W[n_rows
+ * * n] -> REAL x[n]; batched coefficient sets must be packed.
+ *   _dual: x = irfft(sum_r rfft(W_r) * dual_r), DC / Nyquist imaginary parts
+ *          zeroed, 1/n on the inverse; dual: the bank's dual rows (the
+ *          reference's psi_r / (sum_r psi_r^2 + eps), n/2+1 weights per row,
+ *          dual_stride floats apart, host or device pointer).
+ *   _l1:   x = (sum over the wavelet rows of W_r * dlog) / C, plus row 0
+ *          when has_lowpass; dlog = ln 2 / voices, C the bank report's
+ *          admissibility_C (C <= 0 is taken as 1). */
+faf_transform *faf_cuda_create_icwt_dual(size_t n, size_t n_rows, const float *dual,
+                                         size_t dual_stride);
+faf_transform *faf_cuda_create_icwt_l1(size_t n, size_t n_rows, int has_lowpass, double dlog,
+                                       double C);
+
 /* ---- uneven batches (one persistent launch) ------------------------------- */
 
 typedef struct faf_uneven faf_uneven;

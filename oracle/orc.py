@@ -172,6 +172,47 @@ def cwt(x, psi):
     return c2r(Yr, Yi, n)
 
 
+def cwt_dual(psi, eps=1e-6):
+    """Dual-frame rows of a bank (src/faf_cwt.c:440-482): psi_r / (sum_r
+    psi_r^2 + eps), the sum in FP64, zero where it is 0."""
+    p = np.asarray(psi, np.float64)
+    s = np.sum(p * p, axis=0)
+    return np.where(s > 0, p / (s + eps), 0.0).astype(np.float32)
+
+
+def icwt_dual(W, dual):
+    """Dual-frame inverse CWT (src/faf_cwt.c:935-985): the R2C of every row,
+    acc = sum over rows (in order) of Y_r * dual_r, DC / Nyquist imaginary
+    parts zeroed, then the C2R (1/n).  W (batch, rows, n) -> (batch, n)."""
+    W = _f32(W)
+    n = W.shape[-1]
+    Yr, Yi = r2c(W)
+    d = _f32(dual)
+    ar = np.zeros(Yr.shape[:-2] + Yr.shape[-1:], np.float32)
+    ai = np.zeros_like(ar)
+    for r in range(W.shape[-2]):
+        ar += Yr[..., r, :] * d[r]
+        ai += Yi[..., r, :] * d[r]
+    ai[..., 0] = 0.0
+    ai[..., -1] = 0.0
+    return c2r(ar, ai, n)
+
+
+def icwt_l1(W, has_lowpass, dlog, C):
+    """L1 one-integral inverse CWT (src/faf_cwt.c:879-930), FP32 in the
+    reference's order."""
+    W = _f32(W)
+    lo = 1 if has_lowpass else 0
+    acc = np.zeros(W.shape[:-2] + W.shape[-1:], np.float32)
+    dl = np.float32(dlog)
+    for r in range(lo, W.shape[-2]):
+        acc += W[..., r, :] * dl
+    acc /= np.float32(C if C > 0 else 1.0)
+    if has_lowpass:
+        acc += W[..., 0, :]
+    return acc
+
+
 def fp64_cwt(x, psi):
     """The same bank in FP64 numpy."""
     n = x.shape[-1]

@@ -36,7 +36,7 @@ static void drv_fail(const char *what) {
     snprintf(g_drv_err, sizeof(g_drv_err), "%s: %s", what, faf_get_error());
 }
 
-typedef enum { JOB_C2C, JOB_R2C, JOB_C2R, JOB_PIPE, JOB_STFT, JOB_CWT } job_kind;
+typedef enum { JOB_C2C, JOB_R2C, JOB_C2R, JOB_PIPE, JOB_STFT, JOB_CWT, JOB_ICWT } job_kind;
 
 typedef struct {
     job_kind kind;
@@ -77,6 +77,10 @@ static faf_transform *make_transform(const job *j) {
         /* The reference's default bank (Morse 20/3, L1, 10 voices, lowpass). */
         faf_cwt_config cc = faf_cwt_config_init(j->n);
         return faf_create_cwt(&cc);
+    }
+    case JOB_ICWT: {
+        faf_cwt_config cc = faf_cwt_config_init(j->n);
+        return faf_create_icwt(&cc, (faf_cwt_inverse_kind)j->inverse);
     }
     case JOB_PIPE: {
         faf_transform *t = chirp_compile(j->src);
@@ -137,6 +141,11 @@ static void *run_job(void *arg) {
         case JOB_CWT:
             in = faf_buffer_real((void *)(j->in_re + b * n), n);
             out = faf_buffer_real(j->out_re + b * j->rows * n, j->rows * n);
+            rc = faf_execute(t, &out, &in);
+            break;
+        case JOB_ICWT:
+            in = faf_buffer_real((void *)(j->in_re + b * j->rows * n), j->rows * n);
+            out = faf_buffer_real(j->out_re + b * n, n);
             rc = faf_execute(t, &out, &in);
             break;
         case JOB_STFT: {
@@ -274,6 +283,31 @@ int refdrv_cwt_bank(size_t n, size_t *n_rows, size_t *n_bins, int *has_lowpass, 
     }
     faf_destroy_transform(t);
     return 0;
+}
+
+/* The default bank's inverse constants: admissibility C from its report
+ * (faf_cwt_bank_report, include/fastandfourier.h:785) and voices per octave. */
+int refdrv_cwt_consts(size_t n, double *C, unsigned *voices) {
+    faf_cwt_config cc = faf_cwt_config_init(n);
+    faf_transform *t = faf_create_cwt(&cc);
+    if (!t) { drv_fail("cwt create"); return -1; }
+    const faf_cwt_lp_report *r = faf_cwt_bank_report(t);
+    if (C) *C = r ? r->admissibility_C : 0.0;
+    if (voices) *voices = cc.voices;
+    faf_destroy_transform(t);
+    return 0;
+}
+
+/* Inverse CWT (kind: FAF_CWT_INV_DUAL or FAF_CWT_INV_L1) of `batch`
+ * coefficient sets W [batch][rows][n] -> x [batch][n], default bank. */
+int refdrv_icwt(size_t n, int kind, size_t batch, const float *W, float *x, int nthreads) {
+    size_t rows = 0;
+    if (refdrv_cwt_bank(n, &rows, NULL, NULL, NULL) != 0) return -1;
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_ICWT; j.n = n; j.rows = rows; j.inverse = kind;
+    j.in_re = W; j.out_re = x;
+    return run_batched(&j, batch, nthreads);
 }
 
 /* Forward CWT of `batch` signals with the default bank; W is

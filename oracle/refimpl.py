@@ -77,6 +77,9 @@ def lib():
         szp = ctypes.POINTER(sz)
         L.refdrv_cwt_bank.argtypes = [sz, szp, szp, ctypes.POINTER(i), _f32p]
         L.refdrv_cwt.argtypes = [sz, sz, _f32p, _f32p, i]
+        L.refdrv_cwt_consts.argtypes = [sz, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_uint)]
+        L.refdrv_icwt.argtypes = [sz, i, sz, _f32p, _f32p, i]
         L.refdrv_is_size_supported.argtypes = [i, sz]
         L.refdrv_recommended_size.argtypes = [i, sz]
         L.refdrv_recommended_size.restype = sz
@@ -180,6 +183,23 @@ def cwt(x, threads=1):
     W = np.empty(x.shape[:-1] + (rows, n), np.float32)
     _check(lib().refdrv_cwt(n, x.size // n, _p(x), _p(W), threads))
     return W
+
+
+def cwt_consts(n):
+    """(admissibility C, voices) of the reference's default bank for n."""
+    c, v = ctypes.c_double(), ctypes.c_uint()
+    _check(lib().refdrv_cwt_consts(n, ctypes.byref(c), ctypes.byref(v)))
+    return c.value, v.value
+
+
+def icwt(W, kind=0, threads=1):
+    """The reference's inverse CWT (kind 0 dual frame, 1 L1) of W (batch,
+    rows, n) with its default bank: x (batch, n)."""
+    W = _f32(W)
+    n = W.shape[-1]
+    x = np.empty(W.shape[:-2] + (n,), np.float32)
+    _check(lib().refdrv_icwt(n, kind, x.size // n, _p(W), _p(x), threads))
+    return x
 
 
 def is_size_supported(ttype, n):

@@ -122,6 +122,10 @@ def main():
         psi, _ = refimpl.cwt_bank(n)
         out[f"cwt_psi_{n}"] = psi
         out[f"cwt_{n}"] = refimpl.cwt(cases.real_input(n, batch=1, seed=9))
+        # the inverses of those coefficients, and the L1 inverse's constants
+        out[f"icwt_dual_{n}"] = refimpl.icwt(out[f"cwt_{n}"], 0)
+        out[f"icwt_l1_{n}"] = refimpl.icwt(out[f"cwt_{n}"], 1)
+        out[f"cwt_consts_{n}"] = np.array(refimpl.cwt_consts(n), np.float64)
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
 
     policy = {"supported": {}, "recommended": {}, "create": []}

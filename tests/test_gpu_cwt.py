@@ -114,3 +114,72 @@ def test_cwt_create_errors(cuda):
     with pytest.raises(F.FafError, match="buffer n mismatch"):
         t.execute(F._buf(np.zeros(2 * 64, np.float32), None, 2 * 64, F.L_REAL),
                   F._buf(np.zeros(32, np.float32), None, 32, F.L_REAL))
+
+
+@pytest.mark.parametrize("n", cases.CWT)
+def test_icwt_matches_reference_golden(cuda, n):
+    """Both inverse forms on the reference's coefficients, against the
+    reference's own inverse outputs."""
+    import math
+    import fastandfourier_b200 as F
+    torch = cuda
+    g = np.load(os.path.join(GOLD, "golden.npz"))
+    W, psi = g[f"cwt_{n}"], g[f"cwt_psi_{n}"]
+    C, voices = g[f"cwt_consts_{n}"]
+    td = F.Transform.icwt_dual(n, F.Transform.cwt_dual_rows(psi))
+    assert td.type == F.T_ICWT and td.kind == "icwt-dual"
+    x = td.synthesize(torch.from_numpy(W).cuda()).cpu().numpy()
+    assert rel(x, g[f"icwt_dual_{n}"]) <= REL_L2_TOL
+    tl = F.Transform.icwt_l1(n, psi.shape[0], True, math.log(2) / voices, C)
+    assert tl.kind == "icwt-l1"
+    x = tl.synthesize(torch.from_numpy(W).cuda()).cpu().numpy()
+    assert rel(x, g[f"icwt_l1_{n}"]) <= REL_L2_TOL
+
+
+@pytest.mark.parametrize("n", [256, 1000, 4096, 6000])
+def test_cwt_dual_round_trip(cuda, n):
+    """analyze -> synthesize with the bank's dual rows returns the signal
+    (a tight frame up to eps); batched, against the oracle too."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    psi = bank(24, n, n + 3)
+    psi[0] = np.maximum(psi[0], 1.0 - psi[1:].max(axis=0))  # cover every bin
+    x = seeded(n + 4).standard_normal((5, n)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    W = F.Transform.cwt(n, psi).analyze(xd)
+    dual = F.Transform.cwt_dual_rows(psi)
+    t = F.Transform.icwt_dual(n, dual)
+    y = t.synthesize(W).cpu().numpy()
+    assert rel(y, orc.icwt_dual(W.cpu().numpy(), dual)) <= REL_L2_TOL
+    assert rel(y, x) <= 1e-4
+    assert t.wait_status() == 0
+
+
+def test_icwt_batches_and_host_buffers(cuda):
+    import fastandfourier_b200 as F
+    torch = cuda
+    n, rows = 2048, 9
+    rng = seeded(21)
+    W = rng.standard_normal((3, rows, n)).astype(np.float32)
+    dual = bank(rows, n, 22)
+    want = orc.icwt_dual(W, dual)
+    t = F.Transform.icwt_dual(n, dual)
+    assert rel(t.synthesize(W), want) <= REL_L2_TOL                      # host buffers
+    assert rel(t.synthesize(torch.from_numpy(W).cuda()).cpu().numpy(), want) <= REL_L2_TOL
+    tl = F.Transform.icwt_l1(n, rows, False, 0.0693, 0.5)
+    assert rel(tl.synthesize(torch.from_numpy(W).cuda()).cpu().numpy(),
+               orc.icwt_l1(W, False, 0.0693, 0.5)) <= REL_L2_TOL
+
+
+def test_icwt_large_batch_chunks(cuda):
+    """More coefficient sets than one 64 MB chunk of row spectra."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n, rows, batch = 4096, 16, 260
+    dual = bank(rows, n, 31)
+    W = torch.randn(batch, rows, n, device="cuda")
+    t = F.Transform.icwt_dual(n, dual)
+    y = t.synthesize(W)
+    assert F.lib().faf_cuda_last_launches() == 6
+    pick = [0, 1, 255, 256, 259]
+    assert rel(y[pick].cpu().numpy(), orc.icwt_dual(W[pick].cpu().numpy(), dual)) <= REL_L2_TOL

@@ -179,3 +179,16 @@ def test_oracle_cwt_vs_reference(gold, n):
     got = orc.cwt(x, psi)
     assert orc.rel_l2(got, want) <= TOL
     assert orc.rel_l2(got, orc.fp64_cwt(x, psi)) <= TOL
+
+
+@pytest.mark.parametrize("n", cases.CWT)
+def test_oracle_icwt_vs_reference(gold, n):
+    """The oracle's dual-frame and L1 inverse CWT against the reference's
+    faf_icwt_execute on the reference's own coefficients."""
+    import math
+    W, psi = gold[f"cwt_{n}"], gold[f"cwt_psi_{n}"]
+    C, voices = gold[f"cwt_consts_{n}"]
+    got = orc.icwt_dual(W, orc.cwt_dual(psi))
+    assert orc.rel_l2(got, gold[f"icwt_dual_{n}"]) <= TOL
+    got = orc.icwt_l1(W, True, math.log(2) / voices, C)
+    assert orc.rel_l2(got, gold[f"icwt_l1_{n}"]) <= TOL
