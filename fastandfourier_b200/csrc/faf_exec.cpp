@@ -543,8 +543,8 @@ int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t s
         break;
     case FAF_TRANSFORM_CWT: {
         e = fafp::exec_cwt(p, r.in_a, r.out_a, r.batch, in_dist, out_dist, st);
-        const long long nb = (long long)t->n / 2 + 1;
-        const long long cap = std::max(1LL, std::min(r.batch, (32LL << 20) / (nb * 8)));
+        const long long xd = ((long long)t->n / 2 + 2) & ~1LL;  // exec_cwt's spectrum stride
+        const long long cap = std::max(1LL, std::min(r.batch, (32LL << 20) / (xd * 8)));
         launches = (int)(2 * ((r.batch + cap - 1) / cap));
         break;
     }

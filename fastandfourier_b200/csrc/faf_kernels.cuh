@@ -74,6 +74,13 @@ struct RealArgs {  // R2C / C2R / pipeline / STFT
     int filt_rows;
 };
 
+// Input ring slot of a CWT row in the power-of-two C2R kernel (inner length
+// N): the signal's interleaved spectrum, N + 1 bins rounded up to N + 2, and
+// the bank row, N + 1 weights rounded up to N + 4 (both 16-byte multiples).
+__host__ __device__ constexpr int cwt_slot_x(int N) { return N + 2; }       // float2
+__host__ __device__ constexpr int cwt_slot_psi(int N) { return N + 4; }     // floats
+__host__ __device__ constexpr int cwt_slot_f2(int N) { return N + 2 + (N + 4) / 2; }
+
 // Offsets of C2R transform b: plain, or a CWT row (RealArgs::filt).
 struct C2ROffsets {
     long long io, oo;   // input (elements of in_dist units x fpe) / output float offsets

@@ -236,7 +236,7 @@ void free_size(FftSize& s) {
 // float2 each, at most fafct::kRingMax) and `ring_extra` bytes behind them;
 // fewer than 2 slots means no ring.
 fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int ring,
-                           int target_threads, size_t ring_extra) {
+                           int target_threads, size_t ring_extra, size_t slot_bytes) {
     fafk::Geometry g;
     g.E = kE;
     const int T = s.n / 16;
@@ -258,7 +258,7 @@ fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int rin
     // group in warps of its own (T >= 32): groups sharing a warp synchronise
     // with warp barriers across the whole warp.
     if (ring > 0 && T >= 32) {
-        const size_t slot = (size_t)s.n * sizeof(float2);
+        const size_t slot = slot_bytes ? slot_bytes : (size_t)s.n * sizeof(float2);
         const size_t used = g.smem + table + kRingStatic + ring_extra;
         int K = used < kMaxSmem ? (int)((kMaxSmem - used) / slot) : 0;
         // FAF_CUDA_RING=k: k slots where they fit (k < 2: no ring)
@@ -957,23 +957,34 @@ cudaError_t exec_icwt(DevicePlan* p, const float* W, float* x, long long batch, 
 cudaError_t exec_cwt(DevicePlan* p, const float* x, float* W, long long batch, long long in_dist,
                      long long out_dist, cudaStream_t st) {
     const long long nb = p->n / 2 + 1;
-    const long long cap = std::max(1LL, std::min(batch, (32LL << 20) / (nb * 8)));
+    // spectra interleaved, rows an even number of bins apart (16-byte aligned)
+    const long long xd = (nb + 1) & ~1LL;
+    const long long cap = std::max(1LL, std::min(batch, (32LL << 20) / (xd * 8)));
     float* spec = nullptr;
-    cudaError_t e0 = plan_scratch(p, (size_t)cap * (size_t)nb * 2 * sizeof(float), &spec);
+    cudaError_t e0 = plan_scratch(p, (size_t)cap * (size_t)xd * 2 * sizeof(float), &spec);
     if (e0 != cudaSuccess) return e0;
-    float* Xr = spec;
-    float* Xi = spec + cap * nb;
     for (long long s0 = 0; s0 < batch; s0 += cap) {
         const long long c = std::min(cap, batch - s0);
-        cudaError_t e = exec_r2c(p, x + s0 * in_dist, Xr, Xi, c, in_dist, nb, false, st);
+        cudaError_t e = exec_r2c(p, x + s0 * in_dist, spec, nullptr, c, in_dist, xd, true, st);
         if (e != cudaSuccess) return e;
         fafk::RealArgs a = real_args(p, c * p->rows);
         a.scale = p->scale2;
-        a.in_a = Xr; a.in_b = Xi; a.out_a = W + s0 * out_dist;
-        a.in_dist = nb; a.out_dist = out_dist;
+        a.in_a = spec; a.in_b = nullptr; a.interleaved = 1; a.out_a = W + s0 * out_dist;
+        a.in_dist = xd; a.out_dist = out_dist;
         a.filt = p->d_psi; a.filt_dist = p->psi_dist; a.filt_rows = p->rows;
         a.row_len = p->n;
-        if ((e = launch_c2r_args(p, a, c * p->rows, st)) != cudaSuccess) return e;
+        const int N = p->inner.n;
+        if (p->inner.ct_log2 && !p->large && xd == fafk::cwt_slot_x(N) &&
+            p->psi_dist == fafk::cwt_slot_psi(N) && ring_ok(spec, 2 * xd)) {
+            // spectrum and bank row of every row transform land in the ring
+            e = fafk::launch_pot2(2, p->inner.ct_log2, p->inner.d_tws, &a,
+                                  geometry_ct(p->inner, N + 1, c * p->rows, fafct::kRingMax, 1024,
+                                              0, (size_t)fafk::cwt_slot_f2(N) * sizeof(float2)),
+                                  st);
+        } else {
+            e = launch_c2r_args(p, a, c * p->rows, st);
+        }
+        if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
 }

@@ -18,6 +18,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 namespace fafct {
 
@@ -127,11 +128,19 @@ struct Ring {
     }
 };
 
+// A transform's input in two parts (the second may be empty).
+struct RingSrc2 {
+    const void* p0;
+    const void* p1;
+};
+
 // Whole CTA: barriers, issue counters, and the first K copies (issued by
-// threads 0..K-1; src(b) is transform b's input, copied as `bytes`).
+// threads 0..K-1; src(b) is transform b's input: a pointer copied as
+// `bytes`, or a RingSrc2 copied as bytes then bytes1).
 template <class SrcOf>
 __device__ __forceinline__ Ring ring_start(RingCtl* ctl, float2* slots, int K, int slot_f2, int G,
-                                           long long batch, const SrcOf& src, unsigned bytes) {
+                                           long long batch, const SrcOf& src, unsigned bytes,
+                                           unsigned bytes1 = 0) {
     Ring r{ctl, slots, K, slot_f2, G};
     if (threadIdx.x < (unsigned)K) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&ctl->bar[threadIdx.x]))
@@ -143,7 +152,13 @@ __device__ __forceinline__ Ring ring_start(RingCtl* ctl, float2* slots, int K, i
     __syncthreads();
     if (threadIdx.x < (unsigned)K) {
         const long long b = r.transform(threadIdx.x);
-        if (b < batch) r.issue(threadIdx.x, 0, src(b), bytes);
+        if (b < batch) {
+            const auto p = src(b);
+            if constexpr (std::is_same_v<std::decay_t<decltype(p)>, RingSrc2>)
+                r.issue(threadIdx.x, 0, p.p0, bytes, p.p1, bytes1);
+            else
+                r.issue(threadIdx.x, 0, p, bytes);
+        }
     }
     return r;
 }

@@ -254,27 +254,68 @@ __global__ void __launch_bounds__(1024) k2_stft(const float2* __restrict__ tws, 
 }
 
 template <int N>
+struct CwtSlot {
+    static constexpr int X = cwt_slot_x(N);      // float2
+    static constexpr int PSI = cwt_slot_psi(N);  // floats
+    static constexpr int F2 = cwt_slot_f2(N);    // float2 per slot
+};
+
+// RING (CWT rows only: interleaved spectra N + 2 bins apart, bank rows N + 4
+// floats apart): each transform's spectrum and bank row land in the CTA's
+// ring by two bulk copies; otherwise the pair loop loads them.
+template <int N, bool RING>
 __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, const RealArgs a,
-                                               int G, bool vec) {
+                                               int G, bool vec, int K) {
     extern __shared__ float4 smem4[];
     constexpr int nc = N, T = P2<N>::T;
-    CtGroup<N> q(reinterpret_cast<float2*>(smem4), N + 1, tws);
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    CtGroup<N> q(sm, N + 1, tws);
     const SmemC mid{q.ws};
     const int fpe = a.interleaved ? 2 : 1;
+    using CS = CwtSlot<N>;
+    // the two parts of transform b's ring copy
+    auto cwt_src = [&](long long b) {
+        const long long s = b / a.filt_rows, row = b - s * a.filt_rows;
+        return fafct::RingSrc2{a.in_a + s * a.in_dist * 2, a.filt + row * a.filt_dist};
+    };
+    fafct::Ring R{};
+    fafct::RingCursor c{};
+    int dnext = 0;
+    if constexpr (RING) {
+        __shared__ fafct::RingCtl ctl;
+        R = fafct::ring_start(&ctl, ring_base<N>(sm, G, N + 1), K, CS::F2, G, a.batch, cwt_src,
+                              CS::X * 8u, CS::PSI * 4u);
+        c = R.cursor(q.g);
+        dnext = R.next_offset(q.g);
+    }
+    bool first = true;
     CT_FOR_GROUPS(G, a.batch) {
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
         const C2ROffsets o = c2r_offsets(a, bi, fpe);
         const long long io = o.io;
+        const float2* xs = nullptr;  // RING: the slot's spectrum, then its bank row
+        if constexpr (RING) {
+            if (!first) R.advance(c);
+            first = false;
+            if (live && !R.wait(c) && q.t == 0) R.fail(a.err);
+            xs = R.slot_ptr(c);
+        }
         q.sync();  // the previous transform's last stage may still read ws
         // bin k of the input, times the bank's real weight for a CWT row
         // (src/faf_cwt_kernels.c:22-33; the imaginary parts of DC and Nyquist,
         // which that kernel zeroes, are never read by the pre-pass)
         auto load = [&](int k) {
             cf v;
+            if constexpr (RING) {
+                const float2 u = xs[k];
+                const float w = reinterpret_cast<const float*>(xs + CS::X)[k];
+                return cf{u.x * w, u.y * w};
+            }
             if (a.interleaved) {
-                const float2 u = __ldcs(reinterpret_cast<const float2*>(a.in_a + io) + k);
+                const float2* p = reinterpret_cast<const float2*>(a.in_a + io) + k;
+                const float2 u = o.f ? __ldg(p) : __ldcs(p);
                 v = cf{u.x, u.y};
             } else {
                 // a CWT spectrum is re-read by every row of its signal: keep it cached
@@ -291,22 +332,39 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
         // each thread loads whole bin pairs (k, nc - k) and runs the pre-pass
         // on them in registers: one workspace write per bin
         if (live) {
-            for (int k = q.t; k <= nc / 2; k += T) {
-                const cf xk = load(k), xn = load(nc - k);
-                if (k == 0) {
-                    mid.put(0, cf{xk.x + xn.x, xk.x - xn.x});
-                } else {
-                    cf Zk, Znk;
-                    c2r_pair(xk, xn, __ldg(&a.stw[k - 1]), Zk, Znk);
-                    if (k != nc - k) mid.put(k, Zk);
-                    mid.put(nc - k, Znk);
+            // a compile-time trip count lets the loads of every pair issue
+            // before the first one returns (they come from L2 for CWT rows)
+            constexpr int MP = (nc / 2 + T) / T;
+#pragma unroll
+            for (int i = 0; i < MP; i++) {
+                const int k = q.t + i * T;
+                if (k <= nc / 2) {
+                    const cf xk = load(k), xn = load(nc - k);
+                    if (k == 0) {
+                        mid.put(0, cf{xk.x + xn.x, xk.x - xn.x});
+                    } else {
+                        cf Zk, Znk;
+                        c2r_pair(xk, xn, __ldg(&a.stw[k - 1]), Zk, Znk);
+                        if (k != nc - k) mid.put(k, Zk);
+                        mid.put(nc - k, Znk);
+                    }
                 }
             }
         }
         q.sync();
+        if constexpr (RING) {
+            // every thread of the group has read the slot: load the group's
+            // transform K sequence places on into it
+            const long long bn = b + dnext;
+            if (q.t == 0 && live && bn < a.batch) {
+                const fafct::RingSrc2 p = cwt_src(bn);
+                R.issue(c.slot, c.use + 1, p.p0, CS::X * 8u, p.p1, CS::PSI * 4u);
+            }
+        }
         ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
                           RealPairSink{a.out_a + o.oo, a.scale, live, vec}, q.sync);
     }
+    if constexpr (RING) fafct::ring_drain(R);
 }
 
 // Per bin pair of the pipeline: post-pass -> ops -> pre-pass, in registers,
@@ -489,9 +547,16 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     }
     case 2: {
         const RealArgs& a = *(const RealArgs*)args;
-        if ((e = prep(k2_c2r<N>, g.smem)) != cudaSuccess) return e;
-        k2_c2r<N><<<persistent_grid(k2_c2r<N>, g, a.batch), g.threads, g.smem, st>>>(
-            tws, a, g.G, vec_ok(a.out_a, a.out_dist));
+        if (kRingN<N> && g.ring) {
+            if ((e = prep(k2_c2r<N, kRingN<N>>, g.smem)) != cudaSuccess) return e;
+            k2_c2r<N, kRingN<N>><<<persistent_grid(k2_c2r<N, kRingN<N>>, g, a.batch), g.threads,
+                                   g.smem, st>>>(tws, a, g.G, vec_ok(a.out_a, a.out_dist),
+                                                 g.ring);
+        } else {
+            if ((e = prep(k2_c2r<N, false>, g.smem)) != cudaSuccess) return e;
+            k2_c2r<N, false><<<persistent_grid(k2_c2r<N, false>, g, a.batch), g.threads, g.smem,
+                               st>>>(tws, a, g.G, vec_ok(a.out_a, a.out_dist), 0);
+        }
         break;
     }
     case 3: {

@@ -52,7 +52,8 @@ __global__ void __launch_bounds__(1024) k_c2r(const Shape S, const float2* __res
         cf v{0.f, 0.f};
         if (live) {
             if (a.interleaved) {
-                float2 u = __ldcs(reinterpret_cast<const float2*>(a.in_a + io) + k);
+                const float2* p = reinterpret_cast<const float2*>(a.in_a + io) + k;
+                const float2 u = o.f ? __ldg(p) : __ldcs(p);
                 v = cf{u.x, u.y};
             } else {
                 v = o.f ? cf{__ldg(a.in_a + io + k), __ldg(a.in_b + io + k)}
