@@ -11,7 +11,7 @@ of the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload pipeline|r2c|c2c1024|c2c16384|c2c16384tc|c2c4096fp64|
-                                stft|istft|cwt|uneven|serve]
+                                stft|istft|cwt|icwt|uneven|serve]
 
 --workload serve replays a Poisson request trace (20k requests/s: 40% rfft
 of log-uniform sizes 256..65536 rounded to the recommended size, 30% the
@@ -102,6 +102,10 @@ def cwt_bank(rows=CWT_ROWS, n=4096, seed=6):
     return (g * np.exp(-0.5 * ((k - c) / (0.2 * c + 1.0)) ** 2)).astype(np.float32)
 
 
+WORKLOADS["icwt"] = ("inverse CWT (dual frame) n=4096: 256 coefficient sets x 60 rows -> 256 "
+                     "signals (dual rows of the synthetic bank, seed 6), N(0,1) coefficients, "
+                     "seed 7", 4096, 256, 4 * 4096 * (1 + CWT_ROWS), None)
+
 WORKLOADS["serve"] = ("serving trace: 4000 requests, Poisson 20k req/s (seed 4); 40% rfft "
                       "N log-uniform [256, 65536] -> recommended size, 30% notch pipeline "
                       "4096, 30% STFT Hann 1024 hop 256 over L log-uniform [2^16, 2^20]; "
@@ -145,6 +149,8 @@ def make_inputs(workload, batch):
         return [rng.standard_normal((batch, 1 << 18), dtype=np.float32)]
     if workload == "cwt":
         return [np.random.default_rng(5).standard_normal((batch, n), dtype=np.float32)]
+    if workload == "icwt":
+        return [np.random.default_rng(7).standard_normal((batch, CWT_ROWS, n), dtype=np.float32)]
     if workload == "uneven":
         total = sum(uneven_lengths(batch))
         rng = np.random.default_rng(2)
@@ -269,6 +275,8 @@ def build_transform(F, workload, torch):
         return F.Transform.istft(1024, win=1024, hop=256)
     if workload == "cwt":
         return F.Transform.cwt(4096, cwt_bank())
+    if workload == "icwt":
+        return F.Transform.icwt_dual(4096, F.Transform.cwt_dual_rows(cwt_bank()))
     if workload.startswith("c2c"):
         return F.Transform.fft(n)
     if workload == "stft":
@@ -291,6 +299,8 @@ def run_step(F, t, workload, ins, outs, plain=False):
         t.istft_frames(ins[0], ins[1], out=outs[0])
     elif workload == "cwt":
         t.analyze(ins[0], out=outs[0])
+    elif workload == "icwt":
+        t.synthesize(ins[0], out=outs[0])
     elif workload == "uneven":
         if hasattr(ins[0], "data_ptr"):
             t.execute(ins[0], ins[1], outs[0], outs[1], plain=plain)
@@ -332,6 +342,8 @@ def alloc_outputs(workload, batch, like, torch):
         return [mk((batch, 1 << 18))]
     if workload == "cwt":
         return [mk((batch, CWT_ROWS, n))]
+    if workload == "icwt":
+        return [mk((batch, n))]
     if workload == "uneven":
         total = sum(uneven_lengths(batch))
         return [mk((total,)), mk((total,))]
@@ -486,7 +498,8 @@ def run_ours(args, rank, world, local_rank):
                 "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
                            "uneven": "k_uneven_large", "c2c16384tc": "k2_c2c_tc",
                            "c2c4096fp64": "k64_c2c", "istft": "k2_c2r + k_ola",
-                           "cwt": "k2_c2r (bank rows) + k2_r2c"}.get(
+                           "cwt": "k2_c2r (bank rows) + k2_r2c",
+                           "icwt": "k2_r2c (rows) + k_icwt_acc + k2_c2r"}.get(
                                workload, "k2_c2c")}
 
     cpu = None
@@ -569,6 +582,8 @@ def _ref_call(refimpl, workload, sample_inputs, threads):
     elif workload == "cwt":
         # the reference's own bank at this n (60 rows, as the timed bank)
         refimpl.cwt(sample_inputs[0], threads=threads)
+    elif workload == "icwt":
+        refimpl.icwt(sample_inputs[0], 0, threads=threads)
     elif workload == "uneven":
         # sample_inputs: (re, im, lengths) ragged; one reference batch per length
         re, im, lengths = sample_inputs
@@ -617,7 +632,7 @@ def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
         want = max(1, min(want, threads))
     elif workload == "istft":
         want = 2
-    elif workload == "cwt":
+    elif workload in ("cwt", "icwt"):
         want = max(1, min(want, 2 * threads))
     elif workload == "uneven":
         want = 512
@@ -662,6 +677,8 @@ def run_reference(args, rank, world):
         want = min(batch, max(threads * 4, 64))
     if workload == "istft":
         want, threads = 2, 1  # the single-core oracle restatement
+    if workload in ("cwt", "icwt"):
+        want = min(batch, 2 * threads)  # 60 rows per signal: a small sample per step
     sample, nbytes, sample_b = cpu_sample(workload, host_in, want)
     for _ in range(max(args.warmup, 1)):
         _ref_call(refimpl, workload, sample, threads)

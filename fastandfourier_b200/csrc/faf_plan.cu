@@ -235,6 +235,17 @@ void free_size(FftSize& s) {
 // memory left after the workspaces holds up to `ring` input ring slots (n
 // float2 each, at most fafct::kRingMax) and `ring_extra` bytes behind them;
 // fewer than 2 slots means no ring.
+static int device_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    return sms;
+}
+
 fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int ring,
                            int target_threads, size_t ring_extra, size_t slot_bytes) {
     fafk::Geometry g;
@@ -247,7 +258,9 @@ fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int rin
     int target = target_threads;
     if (const char* env = std::getenv("FAF_CUDA_CTA_THREADS")) target = std::max(1, atoi(env));
     int G = std::max(1, target / T);
-    G = (int)std::min<long long>(G, std::max(1LL, batch));
+    // a small batch spreads over every SM (one transform per group, as many
+    // CTAs as SMs allow) instead of filling a few wide CTAs
+    G = (int)std::min<long long>(G, std::max(1LL, batch / device_sms()));
     // groups of >= 32 threads synchronise on named barriers 1..15
     if (T >= 32) G = std::min(G, 15);
     while (G > 1 && ((size_t)G * per + table > kMaxSmem || G * T > 1024)) G--;
