@@ -150,7 +150,8 @@ cudaError_t launch_bluestein(const fafd::Shape& S, const Geometry& g, const floa
 cudaError_t launch_pot2(int kind, int log2n, const float2* tws, const void* args,
                         const Geometry& g, cudaStream_t st);
 // Shared-memory bytes the twiddle table of a log2n kernel adds to each CTA.
-size_t pot2_table_smem(int log2n);
+// twiddle-table bytes of the compile-time kernels; ord: radix order (0 C2C, 1 real kinds)
+size_t pot2_table_smem(int log2n, int ord = 0);
 // Kernel attributes of the compile-time C2C kernel for geometry g (before any
 // stream capture reaches its launch).
 cudaError_t prepare_pot2_c2c(int log2n, const Geometry& g);

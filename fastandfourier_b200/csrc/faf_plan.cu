@@ -1,6 +1,7 @@
 // faf_plan.cu -- planner: radix programs, FP64 tables, launch geometry and
 // device-pointer execution for every plan kind.
 #include "faf_plan.h"
+#include "faf_pot2.cuh"
 #include "faf_ring.cuh"
 
 #include <cuda_fp16.h>
@@ -160,7 +161,7 @@ int plane_floats(int slots) {
     return (p + 1) & ~1;
 }
 
-bool build_size(int n, FftSize& out, std::string& err) {
+bool build_size(int n, FftSize& out, std::string& err, int ct_ord) {
     out = FftSize();
     out.n = n;
     std::vector<int> rad;
@@ -192,15 +193,15 @@ bool build_size(int n, FftSize& out, std::string& err) {
     const char* gen = std::getenv("FAF_CUDA_GENERIC");
     const bool force_generic = gen && gen[0] == '1';
     if (!force_generic && n >= 16 && n <= kMaxSingleCta && (n & (n - 1)) == 0) {
-        // Per-stage table for the compile-time kernels: radix-16 stages, then
-        // the 8/4/2 remainder; stage s (s >= 1) with span P and radix R holds
-        // W_{PR}^{r k} at [(r - 1) P + k].
+        // Per-stage table for the compile-time kernels, in their radix order
+        // (fafct::ct_radix: the same function the kernels use); stage s
+        // (s >= 1) with span P and radix R holds W_{PR}^{r k} at [(r - 1) P + k].
         int lg = 0;
         while ((1 << lg) < n) lg++;
-        const int n16 = lg / 4, rem = lg % 4, ns = n16 + (rem ? 1 : 0);
+        const int ns = fafct::ct_stages(lg, ct_ord);
         std::vector<float2> tws;
         for (int s = 1; s < ns; s++) {
-            const int R = s < n16 ? 16 : (1 << rem), P = 1 << (4 * s);
+            const int R = fafct::ct_radix(lg, ct_ord, s), P = fafct::ct_span(lg, ct_ord, s);
             for (int r = 1; r < R; r++)
                 for (int k = 0; k < P; k++) {
                     const double a = -2.0 * M_PI * (double)r * (double)k / (double)(P * R);
@@ -211,6 +212,7 @@ bool build_size(int n, FftSize& out, std::string& err) {
         if (!cuda_ok(upload(&out.d_tws, tws.data(), tws.size()), err, "twiddle upload"))
             return false;
         out.ct_log2 = lg;
+        out.ct_ord = ct_ord;
     }
     if (out.stages.empty()) {
         // n == 1: keep a valid pointer for the kernels.
@@ -253,7 +255,7 @@ fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int rin
     const int T = s.n / 16;
     // same layout as k_pot2.cu: even2(plane2(slots)) float2 per group
     const int plane2 = (slots - 1) + ((slots - 1) >> 4) + 1;
-    const size_t table = fafk::pot2_table_smem(s.ct_log2);
+    const size_t table = fafk::pot2_table_smem(s.ct_log2, s.ct_ord);
     const size_t per = (size_t)((plane2 + 1) & ~1) * sizeof(float2);
     int target = target_threads;
     if (const char* env = std::getenv("FAF_CUDA_CTA_THREADS")) target = std::max(1, atoi(env));
@@ -585,7 +587,9 @@ DevicePlan* plan_r2c(int n, bool inverse, float scale, std::string& err) {
     DevicePlan* p = new_plan(inverse ? Kind::C2R : Kind::R2C, n);
     p->inverse = inverse;
     p->scale = scale;
-    const bool ok = needs_four_step(nc) ? build_large(p, nc, err) : build_size(nc, p->inner, err);
+    // real kinds: the radix order that ends in 8 (fused bin-pair passes)
+    const bool ok =
+        needs_four_step(nc) ? build_large(p, nc, err) : build_size(nc, p->inner, err, 1);
     if (!ok || !upload_super_twiddles(p, nc, err)) {
         plan_free(p);
         return nullptr;

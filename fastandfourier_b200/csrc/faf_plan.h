@@ -31,12 +31,13 @@ struct FftSize {
     fafd::Stage* d_stages = nullptr;
     float2* d_tw = nullptr;   // W_n^i, i < n (forward), from FP64
     int ct_log2 = 0;          // > 0: compile-time power-of-two kernels apply
+    int ct_ord = 0;           // their radix order (fafct::ct_radix): 0 C2C, 1 real kinds
     float2* d_tws = nullptr;  // their per-stage table [stage][r-1][k] = W_{PR}^{rk}
     fafd::Shape shape(int slots) const;
 };
 
 bool radix_program(int n, std::vector<int>& radices);
-bool build_size(int n, FftSize& out, std::string& err);
+bool build_size(int n, FftSize& out, std::string& err, int ct_ord = 0);
 void free_size(FftSize& s);
 int plane_floats(int slots);
 fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long batch);

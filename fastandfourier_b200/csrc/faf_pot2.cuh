@@ -24,16 +24,39 @@ using fafd::Dft;
 
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
 
-template <int N>
+// Radix order of a 2^lg-point transform (the one source for kernels and the
+// host's twiddle tables).  Order 0: radix-16 stages, then one 8/4/2 stage.
+// Order 1 ends in radix 8 wherever the remainder allows it at the same stage
+// count (2^1: ..., 16, 4, 8; 2^2: ..., 16, 8, 8), so the real-input kernels can
+// fuse their bin-pair pass into the last stage (fafct::ct_last_pairs).
+__host__ __device__ constexpr int ct_stages(int lg, int ord) {
+    return lg / 4 + (lg % 4 ? 1 : 0) + 0 * ord;
+}
+__host__ __device__ constexpr int ct_radix(int lg, int ord, int s) {
+    const int n16 = lg / 4, rem = lg % 4;
+    if (ord == 1 && n16 >= 1 && (rem == 1 || rem == 2)) {
+        if (s < n16 - 1) return 16;
+        if (s == n16 - 1) return rem == 1 ? 4 : 8;
+        return 8;
+    }
+    return s < n16 ? 16 : (1 << rem);
+}
+__host__ __device__ constexpr int ct_span(int lg, int ord, int s) {
+    int p = 1;
+    for (int j = 0; j < s; j++) p *= ct_radix(lg, ord, j);
+    return p;
+}
+
+template <int N, int ORD = 0>
 struct P2 {
     static_assert(N >= 16 && (N & (N - 1)) == 0, "power of two >= 16");
     static constexpr int LOG = ilog2(N);
     static constexpr int N16 = LOG / 4;
     static constexpr int REM = LOG % 4;
-    static constexpr int NS = N16 + (REM ? 1 : 0);
+    static constexpr int NS = ct_stages(LOG, ORD);
     static constexpr int T = N / 16;                    // threads per transform
-    __host__ __device__ static constexpr int radix(int s) { return s < N16 ? 16 : (1 << REM); }
-    __host__ __device__ static constexpr int span(int s) { return 1 << (4 * s); }
+    __host__ __device__ static constexpr int radix(int s) { return ct_radix(LOG, ORD, s); }
+    __host__ __device__ static constexpr int span(int s) { return ct_span(LOG, ORD, s); }
     __host__ __device__ static constexpr int tw_offset(int s) {
         int o = 0;
         for (int j = 1; j < s; j++) o += (radix(j) - 1) * span(j);
@@ -94,11 +117,11 @@ __device__ __forceinline__ float2* fast_ptr(const T& x) {
     else return x.s.d;
 }
 
-template <int N, int S, bool TWS_SMEM, class Src, class Snk, class Sync>
+template <int N, int S, bool TWS_SMEM, int ORD = 0, class Src, class Snk, class Sync>
 __device__ __forceinline__ void ct_stage(float (&xr)[16], float (&xi)[16], int t,
                                          const float2* __restrict__ tws, const Src& src,
                                          const Snk& snk, const Sync& sync) {
-    using Pl = P2<N>;
+    using Pl = P2<N, ORD>;
     constexpr int R = Pl::radix(S), P = Pl::span(S), NB = N / R, T = Pl::T, MB = 16 / R;
     constexpr int LP = ilog2(P);
     constexpr int OFF = Pl::tw_offset(S);
@@ -188,35 +211,35 @@ struct NoHook {
 // caller runs it, fused with what follows; the stage before it has written
 // the workspace and synchronised).
 template <int N, int S, bool TWS_SMEM, class Src, class Snk, class Sync, class Hook,
-          bool SKIP_LAST = false>
+          bool SKIP_LAST = false, int ORD = 0>
 __device__ __forceinline__ void ct_run(float (&xr)[16], float (&xi)[16], int t, float2* ws,
                                        const float2* __restrict__ tws, const Src& src,
                                        const Snk& snk, const Sync& sync, const Hook& hook) {
-    using Pl = P2<N>;
+    using Pl = P2<N, ORD>;
     static_assert(!SKIP_LAST || Pl::NS >= 2, "a skipped last stage needs an earlier one");
     const SmemC mid{ws};
     const LastC<Snk> last{snk};
     if constexpr (Pl::NS == 1) {
         if constexpr (Src::kSmem) {
-            ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid, sync);
+            ct_stage<N, 0, TWS_SMEM, ORD>(xr, xi, t, tws, src, mid, sync);
             hook();
             for (int i = t; i < N; i += Pl::T) last.put(i, mid.get(i));
         } else {
-            ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, last, sync);
+            ct_stage<N, 0, TWS_SMEM, ORD>(xr, xi, t, tws, src, last, sync);
             sync();
             hook();
         }
     } else if constexpr (S == 0) {
         // stage 0 ends with a barrier: the source is no longer read by anyone
-        ct_stage<N, 0, TWS_SMEM>(xr, xi, t, tws, src, mid, sync);
+        ct_stage<N, 0, TWS_SMEM, ORD>(xr, xi, t, tws, src, mid, sync);
         hook();
-        ct_run<N, 1, TWS_SMEM, SmemC, Snk, Sync, NoHook, SKIP_LAST>(xr, xi, t, ws, tws, mid, snk,
+        ct_run<N, 1, TWS_SMEM, SmemC, Snk, Sync, NoHook, SKIP_LAST, ORD>(xr, xi, t, ws, tws, mid, snk,
                                                                     sync, NoHook());
     } else if constexpr (S == Pl::NS - 1) {
-        if constexpr (!SKIP_LAST) ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, last, sync);
+        if constexpr (!SKIP_LAST) ct_stage<N, S, TWS_SMEM, ORD>(xr, xi, t, tws, mid, last, sync);
     } else {
-        ct_stage<N, S, TWS_SMEM>(xr, xi, t, tws, mid, mid, sync);
-        ct_run<N, S + 1, TWS_SMEM, SmemC, Snk, Sync, NoHook, SKIP_LAST>(xr, xi, t, ws, tws, mid,
+        ct_stage<N, S, TWS_SMEM, ORD>(xr, xi, t, tws, mid, mid, sync);
+        ct_run<N, S + 1, TWS_SMEM, SmemC, Snk, Sync, NoHook, SKIP_LAST, ORD>(xr, xi, t, ws, tws, mid,
                                                                         snk, sync, NoHook());
     }
 }
@@ -224,25 +247,27 @@ __device__ __forceinline__ void ct_run(float (&xr)[16], float (&xi)[16], int t, 
 // Forward FFT of N points (compile time) by the T = N/16 threads of one
 // transform group; `ws` is the group's interleaved workspace, `tws` the
 // per-stage twiddle table (shared memory when TWS_SMEM, else global).
-template <int N, bool TWS_SMEM, class Src, class Snk, class Sync, class Hook = NoHook>
+template <int N, bool TWS_SMEM, int ORD = 0, class Src, class Snk, class Sync,
+          class Hook = NoHook>
 __device__ __forceinline__ void ct_fft(int t, float2* ws, const float2* __restrict__ tws,
                                        const Src& src, const Snk& snk, const Sync& sync,
                                        const Hook& hook = Hook()) {
     float xr[16], xi[16];
     if constexpr (!Src::kSmem) sync();
-    ct_run<N, 0, TWS_SMEM>(xr, xi, t, ws, tws, src, snk, sync, hook);
+    ct_run<N, 0, TWS_SMEM, Src, Snk, Sync, Hook, false, ORD>(xr, xi, t, ws, tws, src, snk, sync,
+                                                             hook);
 }
 
 // Every stage but the last, from a global source; the workspace holds the
 // last stage's input when it returns (synchronised).
-template <int N, bool TWS_SMEM, class Src, class Sync, class Hook = NoHook>
+template <int N, bool TWS_SMEM, int ORD = 0, class Src, class Sync, class Hook = NoHook>
 __device__ __forceinline__ void ct_fft_but_last(int t, float2* ws, const float2* __restrict__ tws,
                                                 const Src& src, const Sync& sync,
                                                 const Hook& hook = Hook()) {
     float xr[16], xi[16];
     if constexpr (!Src::kSmem) sync();
-    ct_run<N, 0, TWS_SMEM, Src, SmemC, Sync, Hook, true>(xr, xi, t, ws, tws, src, SmemC{ws}, sync,
-                                                         hook);
+    ct_run<N, 0, TWS_SMEM, Src, SmemC, Sync, Hook, true, ORD>(xr, xi, t, ws, tws, src, SmemC{ws},
+                                                              sync, hook);
 }
 
 // The last stage of an N-point transform whose last radix is 8 (two
@@ -253,22 +278,22 @@ __device__ __forceinline__ void ct_fft_but_last(int t, float2* ws, const float2*
 // t and NB - t (thread 0: 0 and NB / 2, each paired with itself).  Calls
 // dc(Z[0]) once, and pair(k, Z[k], Z[N - k]) once for every 1 <= k <= N / 2
 // (k = N / 2 paired with itself); all bins it touches are the thread's own.
-template <int N>
+template <int N, int ORD = 0>
 struct LastPairs {
-    using Pl = P2<N>;
+    using Pl = P2<N, ORD>;
     static constexpr int S = Pl::NS - 1;
     static constexpr int R = Pl::radix(S);
     static constexpr bool ok = Pl::NS >= 2 && R == 8;
 };
 
-template <int N, bool TWS_SMEM, class Dc, class Pair>
+template <int N, bool TWS_SMEM, int ORD = 0, class Dc, class Pair>
 __device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
                                               const float2* __restrict__ tws, const Dc& dc,
                                               const Pair& pair) {
-    using Pl = P2<N>;
+    using Pl = P2<N, ORD>;
     constexpr int S = Pl::NS - 1, R = Pl::radix(S), P = Pl::span(S), NB = N / R;
     constexpr int OFF = Pl::tw_offset(S);
-    static_assert(LastPairs<N>::ok && P == NB && Pl::T == NB / 2, "radix-8 last stage");
+    static_assert(LastPairs<N, ORD>::ok && P == NB && Pl::T == NB / 2, "radix-8 last stage");
     const int b[2] = {t, t == 0 ? NB / 2 : NB - t};
     float xr[2][R], xi[2][R];
 #pragma unroll
@@ -276,7 +301,8 @@ __device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
         const float2* p = ws + pad2(b[h]);
 #pragma unroll
         for (int r = 0; r < R; r++) {
-            const float2 v = p[r * (NB + NB / 16)];
+            // pad2(b + r NB) = pad2(b) + r (NB + NB / 16) only when 16 | NB
+            const float2 v = NB % 16 == 0 ? p[r * (NB + NB / 16)] : ws[pad2(b[h] + r * NB)];
             xr[h][r] = v.x;
             xi[h][r] = v.y;
         }

@@ -18,10 +18,10 @@ using fafct::plane2;
 // bulk copies need 16-byte aligned shared-memory destinations.
 __host__ __device__ constexpr int even2(int x) { return (x + 1) & ~1; }
 
-template <int N>
+template <int N, int ORD = 0>
 struct CtCfg {
-    static constexpr bool TW_SMEM = P2<N>::TW * 8 <= 32768;
-    static constexpr int TWN = TW_SMEM ? even2(P2<N>::TW > 0 ? P2<N>::TW : 1) : 0;
+    static constexpr bool TW_SMEM = P2<N, ORD>::TW * 8 <= 32768;
+    static constexpr int TWN = TW_SMEM ? even2(P2<N, ORD>::TW > 0 ? P2<N, ORD>::TW : 1) : 0;
 };
 
 // float2 units of one group's workspace
@@ -29,7 +29,7 @@ __host__ __device__ constexpr int group_stride(int n, int slots) {
     return (void)n, even2(plane2(slots));
 }
 
-template <int N>
+template <int N, int ORD = 0>
 struct CtGroup {
     int g, t;
     float2* ws;
@@ -39,26 +39,27 @@ struct CtGroup {
         constexpr int T = P2<N>::T;
         g = threadIdx.x / T;
         t = threadIdx.x % T;
-        if constexpr (CtCfg<N>::TW_SMEM) {
-            for (int i = threadIdx.x; i < CtCfg<N>::TWN; i += blockDim.x) sm[i] = __ldg(&gtw[i]);
+        if constexpr (CtCfg<N, ORD>::TW_SMEM) {
+            for (int i = threadIdx.x; i < CtCfg<N, ORD>::TWN; i += blockDim.x)
+                sm[i] = __ldg(&gtw[i]);
             tw = sm;
         } else {
             tw = gtw;
         }
-        ws = sm + CtCfg<N>::TWN + (size_t)g * group_stride(N, slots);
+        ws = sm + CtCfg<N, ORD>::TWN + (size_t)g * group_stride(N, slots);
         sync = fafct::GroupSync::make(g, T);
         // publish the twiddle table to the whole CTA once
-        if constexpr (CtCfg<N>::TW_SMEM) __syncthreads();
+        if constexpr (CtCfg<N, ORD>::TW_SMEM) __syncthreads();
     }
 };
 
-template <int N>
-constexpr bool kTw = CtCfg<N>::TW_SMEM;
+template <int N, int ORD = 0>
+constexpr bool kTw = CtCfg<N, ORD>::TW_SMEM;
 
 // First ring slot behind the G group workspaces.
-template <int N>
+template <int N, int ORD = 0>
 __device__ __forceinline__ float2* ring_base(float2* sm, int G, int slots) {
-    return sm + CtCfg<N>::TWN + (size_t)G * group_stride(N, slots);
+    return sm + CtCfg<N, ORD>::TWN + (size_t)G * group_stride(N, slots);
 }
 
 // Persistent loop over transform groups; uniform across the CTA.

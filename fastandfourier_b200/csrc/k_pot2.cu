@@ -21,6 +21,12 @@ using fafct::SmemCConj;
 using fafct::ct_fft;
 using fafct::plane2;
 
+// Radix order of the real-input kernels (R2C, C2R, pipeline, STFT): it ends
+// in radix 8 wherever the length allows, so the R2C post-pass and the
+// pipeline's bin-pair pass fuse with the last stage (fafct::ct_last_pairs).
+// Real plans build their twiddle tables in the same order.
+constexpr int kRO = 1;
+
 // Issues the copy of the transform `src` (sequence s of the CTA's ring) once
 // the group's first stage has read its own slot; one thread of the group.
 struct RingHook {
@@ -39,7 +45,7 @@ template <int N>
 __device__ __forceinline__ fafct::Ring real_ring(fafct::RingCtl* ctl, float2* sm, int G, int K,
                                                  const RealArgs& a) {
     return fafct::ring_start(
-        ctl, ring_base<N>(sm, G, N + 1), K, N, G, a.batch,
+        ctl, ring_base<N, kRO>(sm, G, N + 1), K, N, G, a.batch,
         [&](long long b) { return (const void*)(a.in_a + b * a.in_dist); }, N * 8u);
 }
 
@@ -112,7 +118,7 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
                                                int G, bool vec, int K) {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    CtGroup<N> q(sm, N + 1, tws);
+    CtGroup<N, kRO> q(sm, N + 1, tws);
     const SmemC mid{q.ws};
     const int fpe = a.interleaved ? 2 : 1;
     fafct::Ring R{};
@@ -135,16 +141,16 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        if constexpr (fafct::LastPairs<N>::ok) {
+        if constexpr (fafct::LastPairs<N, kRO>::ok) {
             // last stage fused with the post-pass: no workspace round trip
             if constexpr (RING) {
                 const RingHook hook =
                     ring_next(R, c, b, dnext, live, a.in_a, a.in_dist, a.batch, N * 8u, q.t,
                               a.err);
-                fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)},
+                fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)},
                                                   q.sync, hook);
             } else {
-                fafct::ct_fft_but_last<N, kTw<N>>(
+                fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(
                     q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, q.sync);
             }
             if (live) {
@@ -154,7 +160,7 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
                 // one branch per transform on the layout: a per-store branch
                 // costs the fused stage registers it does not have
                 auto post = [&](const auto& out) {
-                    fafct::ct_last_pairs<N, kTw<N>>(
+                    fafct::ct_last_pairs<N, kTw<N, kRO>, kRO>(
                         q.t, q.ws, q.tw,
                         [&](cf z) {
                             out.put(0, (z.x + z.y) * sc, 0.f);
@@ -178,9 +184,9 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
                 const RingHook hook =
                     ring_next(R, c, b, dnext, live, a.in_a, a.in_dist, a.batch, N * 8u, q.t,
                               a.err);
-                ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)}, mid, q.sync, hook);
+                ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)}, mid, q.sync, hook);
             } else {
-                ct_fft<N, kTw<N>>(q.t, q.ws, q.tw,
+                ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw,
                                   RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid, q.sync);
             }
         }
@@ -202,7 +208,7 @@ __global__ void __launch_bounds__(1024) k2_stft(const float2* __restrict__ tws, 
                                                 int G, int K) {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    CtGroup<N> q(sm, N + 1, tws);
+    CtGroup<N, kRO> q(sm, N + 1, tws);
     const SmemC mid{q.ws};
     const int fpe = a.interleaved ? 2 : 1;
     auto frame = [&](long long b) {
@@ -215,12 +221,12 @@ __global__ void __launch_bounds__(1024) k2_stft(const float2* __restrict__ tws, 
     const float2* wsm = nullptr;
     if constexpr (RING) {
         __shared__ fafct::RingCtl ctl;
-        float2* wbuf = ring_base<N>(sm, G, N + 1) + (size_t)K * N;
+        float2* wbuf = ring_base<N, kRO>(sm, G, N + 1) + (size_t)K * N;
         for (int i = threadIdx.x; i < a.win / 2; i += blockDim.x)
             wbuf[i] = __ldg(reinterpret_cast<const float2*>(a.window) + i);
         wsm = wbuf;  // published by the barrier in ring_start
         R = fafct::ring_start(
-            &ctl, ring_base<N>(sm, G, N + 1), K, N, G, a.batch,
+            &ctl, ring_base<N, kRO>(sm, G, N + 1), K, N, G, a.batch,
             [&](long long b) { return (const void*)frame(b); }, (unsigned)a.win * 4u);
         c = R.cursor(q.g);
         dnext = R.next_offset(q.g);
@@ -233,21 +239,63 @@ __global__ void __launch_bounds__(1024) k2_stft(const float2* __restrict__ tws, 
         if constexpr (RING) {
             if (!first) R.advance(c);
             first = false;
-            const RingHook hook =
-                ring_next_of(R, c, b, dnext, live, a.batch,
-                             [&](long long bn) { return (const void*)frame(bn); },
-                             (unsigned)a.win * 4u, q.t, a.err);
-            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, FrameStageSrc{R.slot_ptr(c), wsm, a.win}, mid,
-                              q.sync, hook);
-        } else {
-            ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, FrameSrc{frame(bi), a.window, a.win, live}, mid,
-                              q.sync);
         }
-        q.sync();
-        if (live) {
-            const long long oo = bi * a.out_dist * fpe;
-            HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo, a.interleaved};
-            ct_r2c_post<N>(q.t, mid, a.stw, out, a.scale);
+        if constexpr (fafct::LastPairs<N, kRO>::ok) {
+            // last stage fused with the post-pass, as in k2_r2c
+            if constexpr (RING) {
+                const RingHook hook =
+                    ring_next_of(R, c, b, dnext, live, a.batch,
+                                 [&](long long bn) { return (const void*)frame(bn); },
+                                 (unsigned)a.win * 4u, q.t, a.err);
+                fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(
+                    q.t, q.ws, q.tw, FrameStageSrc{R.slot_ptr(c), wsm, a.win}, q.sync, hook);
+            } else {
+                fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(
+                    q.t, q.ws, q.tw, FrameSrc{frame(bi), a.window, a.win, live}, q.sync);
+            }
+            if (live) {
+                const long long oo = bi * a.out_dist * fpe;
+                const float sc = a.scale;
+                const float2* __restrict__ stw = a.stw;
+                auto post = [&](const auto& out) {
+                    fafct::ct_last_pairs<N, kTw<N, kRO>, kRO>(
+                        q.t, q.ws, q.tw,
+                        [&](cf z) {
+                            out.put(0, (z.x + z.y) * sc, 0.f);
+                            out.put(N, (z.x - z.y) * sc, 0.f);
+                        },
+                        [&](int k, cf zk, cf zn) {
+                            cf Xk, Xnk;
+                            r2c_pair(zk, zn, __ldg(&stw[k - 1]), Xk, Xnk);
+                            if (k != N - k) out.put(k, Xk.x * sc, Xk.y * sc);
+                            out.put(N - k, Xnk.x * sc, Xnk.y * sc);
+                        });
+                };
+                if (a.interleaved)
+                    post(HermInter{reinterpret_cast<float2*>(a.out_a + oo)});
+                else
+                    post(HermSplit{a.out_a + oo, a.out_b + oo});
+            }
+        } else {
+            if constexpr (RING) {
+                const RingHook hook =
+                    ring_next_of(R, c, b, dnext, live, a.batch,
+                                 [&](long long bn) { return (const void*)frame(bn); },
+                                 (unsigned)a.win * 4u, q.t, a.err);
+                ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw,
+                                            FrameStageSrc{R.slot_ptr(c), wsm, a.win}, mid, q.sync,
+                                            hook);
+            } else {
+                ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw,
+                                            FrameSrc{frame(bi), a.window, a.win, live}, mid,
+                                            q.sync);
+            }
+            q.sync();
+            if (live) {
+                const long long oo = bi * a.out_dist * fpe;
+                HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo, a.interleaved};
+                ct_r2c_post<N>(q.t, mid, a.stw, out, a.scale);
+            }
         }
     }
     if constexpr (RING) fafct::ring_drain(R);
@@ -269,7 +317,7 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
     extern __shared__ float4 smem4[];
     constexpr int nc = N, T = P2<N>::T;
     float2* sm = reinterpret_cast<float2*>(smem4);
-    CtGroup<N> q(sm, N + 1, tws);
+    CtGroup<N, kRO> q(sm, N + 1, tws);
     const SmemC mid{q.ws};
     const int fpe = a.interleaved ? 2 : 1;
     using CS = CwtSlot<N>;
@@ -283,7 +331,7 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
     int dnext = 0;
     if constexpr (RING) {
         __shared__ fafct::RingCtl ctl;
-        R = fafct::ring_start(&ctl, ring_base<N>(sm, G, N + 1), K, CS::F2, G, a.batch, cwt_src,
+        R = fafct::ring_start(&ctl, ring_base<N, kRO>(sm, G, N + 1), K, CS::F2, G, a.batch, cwt_src,
                               CS::X * 8u, CS::PSI * 4u);
         c = R.cursor(q.g);
         dnext = R.next_offset(q.g);
@@ -361,7 +409,7 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
                 R.issue(c.slot, c.use + 1, p.p0, CS::X * 8u, p.p1, CS::PSI * 4u);
             }
         }
-        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
+        ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, SmemCConj{q.ws},
                           RealPairSink{a.out_a + o.oo, a.scale, live, vec}, q.sync);
     }
     if constexpr (RING) fafct::ring_drain(R);
@@ -401,7 +449,7 @@ template <int N, class Ops>
 __device__ __forceinline__ void pipe_middle_fused(int t, float2* ws, const float2* tw,
                                                   const float2* __restrict__ stw, const Ops& ops) {
     const SmemC mid{ws};
-    fafct::ct_last_pairs<N, kTw<N>>(
+    fafct::ct_last_pairs<N, kTw<N, kRO>, kRO>(
         t, ws, tw,
         [&](cf z) {
             const cf x0 = ops(0, cf{z.x + z.y, 0.f});
@@ -427,7 +475,7 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
                                                     const RealArgs a, int G, bool vec, int K) {
     extern __shared__ float4 smem4[];
     float2* sm = reinterpret_cast<float2*>(smem4);
-    CtGroup<N> q(sm, N + 1, tws);
+    CtGroup<N, kRO> q(sm, N + 1, tws);
     const SmemC mid{q.ws};
     fafct::Ring R{};
     if constexpr (RING) {
@@ -449,15 +497,15 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
-        if constexpr (fafct::LastPairs<N>::ok) {
+        if constexpr (fafct::LastPairs<N, kRO>::ok) {
             if constexpr (RING) {
                 const RingHook hook =
                     ring_next(R, c, b, dnext, live, a.in_a, a.in_dist, a.batch, N * 8u, q.t,
                               a.err);
-                fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)},
+                fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)},
                                                   q.sync, hook);
             } else {
-                fafct::ct_fft_but_last<N, kTw<N>>(
+                fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(
                     q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, q.sync);
             }
             if (ops_single_mul(a))
@@ -469,9 +517,9 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
                 const RingHook hook =
                     ring_next(R, c, b, dnext, live, a.in_a, a.in_dist, a.batch, N * 8u, q.t,
                               a.err);
-                ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)}, mid, q.sync, hook);
+                ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, fafct::StageSrc{R.slot_ptr(c)}, mid, q.sync, hook);
             } else {
-                ct_fft<N, kTw<N>>(q.t, q.ws, q.tw,
+                ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw,
                                   RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, mid, q.sync);
             }
             q.sync();
@@ -481,7 +529,7 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
                 pipe_middle<N>(q.t, mid, a.stw, OpsAny{&a});
         }
         q.sync();
-        ct_fft<N, kTw<N>>(q.t, q.ws, q.tw, SmemCConj{q.ws},
+        ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, SmemCConj{q.ws},
                           RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec}, q.sync);
     }
     if constexpr (RING) fafct::ring_drain(R);
@@ -515,16 +563,16 @@ static unsigned persistent_grid(K kernel, const Geometry& g, long long batch) {
 template <int N>
 constexpr bool kRingN = N >= 512;
 
-template <int N>
+template <int N, int ORD = 0>
 static size_t tw_bytes() {
-    return (size_t)CtCfg<N>::TWN * sizeof(float2);
+    return (size_t)CtCfg<N, ORD>::TWN * sizeof(float2);
 }
 
 template <int N>
 static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geometry g,
                              cudaStream_t st) {
     cudaError_t e;
-    g.smem += tw_bytes<N>();
+    g.smem += kind == 0 ? tw_bytes<N>() : tw_bytes<N, kRO>();
     switch (kind) {
     case 0: {
         const C2CArgs& a = *(const C2CArgs*)args;
@@ -614,19 +662,14 @@ cudaError_t prepare_pot2_c2c(int log2n, const Geometry& g) {
     }
 }
 
-size_t pot2_table_smem(int log2n) {
-    switch (log2n) {
-    case 4: return tw_bytes<16>();
-    case 5: return tw_bytes<32>();
-    case 6: return tw_bytes<64>();
-    case 7: return tw_bytes<128>();
-    case 8: return tw_bytes<256>();
-    case 9: return tw_bytes<512>();
-    case 10: return tw_bytes<1024>();
-    case 11: return tw_bytes<2048>();
-    case 12: return tw_bytes<4096>();
-    case 13: return tw_bytes<8192>();
-    case 14: return tw_bytes<16384>();
+size_t pot2_table_smem(int log2n, int ord) {
+    switch (log2n * 2 + (ord ? 1 : 0)) {
+#define FAF_TB(L, N)                          \
+    case 2 * L: return tw_bytes<N>();         \
+    case 2 * L + 1: return tw_bytes<N, kRO>();
+        FAF_TB(4, 16) FAF_TB(5, 32) FAF_TB(6, 64) FAF_TB(7, 128) FAF_TB(8, 256) FAF_TB(9, 512)
+        FAF_TB(10, 1024) FAF_TB(11, 2048) FAF_TB(12, 4096) FAF_TB(13, 8192) FAF_TB(14, 16384)
+#undef FAF_TB
     default: return 0;
     }
 }

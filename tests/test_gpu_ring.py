@@ -112,3 +112,21 @@ def test_stft_ring_matches_direct(cuda, monkeypatch, n, win, hop):
     want = np.fft.rfft(fr, axis=-1)
     got = a_re.cpu().numpy() + 1j * a_im.cpu().numpy()
     assert rel(got, want) <= REL_L2_TOL
+
+
+@pytest.mark.parametrize("n", [32, 64, 128, 256, 1024, 2048, 16384, 32768])
+def test_pipeline_sizes_fused_middle(cuda, n):
+    """The pipeline's bin-pair pass fused into the forward FFT's last stage
+    at every length whose real-kind radix order ends in 8, and the unfused
+    pass elsewhere, against FP64 numpy."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    nb = n // 2 + 1
+    rng = seeded(n + 17)
+    x = rng.standard_normal((9, n)).astype(np.float32)
+    m = rng.uniform(0, 1, nb).astype(np.float32)
+    t = F.Transform.chirp(f"(pipeline (rfft :size {n}) (mul-spectrum) (irfft))")
+    t.bind(torch.from_numpy(m).cuda(), torch.zeros(nb, device="cuda"), nb)
+    y = t.pipeline(torch.from_numpy(x).cuda()).cpu().numpy()
+    want = np.fft.irfft(np.fft.rfft(x.astype(np.float64), axis=-1) * m, n=n, axis=-1)
+    assert rel(y, want) <= REL_L2_TOL
