@@ -11,6 +11,12 @@
 // fused into the sources / sinks of those stages.
 #pragma once
 
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <utility>
+
 #include "faf_device.cuh"
 #include "faf_kernels.cuh"
 
@@ -141,14 +147,62 @@ struct RealPairSink {
 // Launch helpers
 // ---------------------------------------------------------------------------
 
+// Host memo of per-kernel launch facts (the shared-memory opt-in made so far,
+// resident CTAs per launch shape), per device, so that a launch after the
+// first costs no driver query: small launches are bound by host time.
+struct LaunchMemo {
+    std::mutex mu;
+    std::map<std::pair<const void*, int>, size_t> smem;                // opted-in bytes
+    std::map<std::tuple<const void*, int, int, size_t>, int> per_sm;  // occupancy
+    static LaunchMemo& get() {
+        static LaunchMemo m;
+        return m;
+    }
+};
+
 template <class K>
 inline cudaError_t prep(K kernel, size_t smem) {
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
+    if (smem <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    LaunchMemo& m = LaunchMemo::get();
+    const auto key = std::make_pair((const void*)kernel, dev);
+    {
+        std::lock_guard<std::mutex> lk(m.mu);
+        auto it = m.smem.find(key);
+        if (it != m.smem.end() && it->second >= smem) return cudaSuccess;
     }
+    cudaError_t e =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(m.mu);
+    size_t& v = m.smem[key];
+    v = std::max(v, smem);
     return cudaSuccess;
+}
+
+// Resident CTAs per SM of `kernel` at this shape (memoised; 1 if the query fails).
+template <class K>
+inline int resident_ctas(K kernel, int threads, size_t smem) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    LaunchMemo& m = LaunchMemo::get();
+    const auto key = std::make_tuple((const void*)kernel, dev, threads, smem);
+    {
+        std::lock_guard<std::mutex> lk(m.mu);
+        auto it = m.per_sm.find(key);
+        if (it != m.per_sm.end()) return it->second;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
+            cudaSuccess ||
+        per_sm <= 0) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    std::lock_guard<std::mutex> lk(m.mu);
+    m.per_sm[key] = per_sm;
+    return per_sm;
 }
 
 inline unsigned grid_for(long long batch, int G) {

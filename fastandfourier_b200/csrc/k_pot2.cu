@@ -548,11 +548,7 @@ static unsigned persistent_grid(K kernel, const Geometry& g, long long batch) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if (sms <= 0) sms = 1;
     }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, g.threads, g.smem) !=
-            cudaSuccess ||
-        per_sm <= 0)
-        per_sm = 1;
+    const int per_sm = resident_ctas(kernel, g.threads, g.smem);
     const long long groups = (batch + g.G - 1) / g.G;
     const long long cap = (long long)sms * per_sm;
     return (unsigned)std::max(1LL, std::min(groups, cap));
