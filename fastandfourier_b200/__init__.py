@@ -72,12 +72,7 @@ def _ptr(a):
 
 
 def _buf(re, im, n, layout):
-    b = C.faf_buffer()
-    b.re = _ptr(re)
-    b.im = _ptr(im)
-    b.n = n
-    b.layout = layout
-    return b
+    return C.faf_buffer(_ptr(re), _ptr(im), n, layout)
 
 
 CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy: the legacy default stream as an explicit handle
@@ -248,6 +243,10 @@ class Transform:
             raise FafError(C.error())
         self._p = ptr
         self._keep = list(keep)
+        # fixed at create: read once, not through ctypes on every call
+        self._n = ptr.contents.n
+        self._inter = ptr.contents.cfg.layout == L_INTERLEAVED
+        self._xb = C.lib().faf_execute_batched
 
     # ---- constructors (reference names) ----
     @classmethod
@@ -337,7 +336,7 @@ class Transform:
 
     @property
     def n(self):
-        return self.s.n
+        return self._n
 
     @property
     def type(self):
@@ -383,14 +382,14 @@ class Transform:
         _check(C.lib().faf_execute(self._p, ctypes.byref(out), ctypes.byref(inp)))
 
     def execute_batched(self, out, inp, batch, in_dist=0, out_dist=0):
-        _check(C.lib().faf_execute_batched(self._p, ctypes.byref(out), ctypes.byref(inp),
-                                           batch, in_dist, out_dist))
+        if self._xb(self._p, ctypes.byref(out), ctypes.byref(inp), batch, in_dist, out_dist):
+            raise FafError(C.error())
 
     def c2c(self, re, im=None, out_re=None, out_im=None):
         """Batched C2C over the last axis.  Split planes (re, im) or one
         interleaved buffer (re only, shape (..., 2n)) for INTERLEAVED plans."""
         n = self.n
-        inter = self.s.cfg.layout == L_INTERLEAVED
+        inter = self._inter
         lay = L_INTERLEAVED if inter else L_SPLIT
         batch = (re.numel() if hasattr(re, "numel") else re.size) // (2 * n if inter else n)
         if out_re is None:
@@ -403,7 +402,7 @@ class Transform:
         n, nb = self.n, self.n // 2 + 1
         batch = (x.numel() if hasattr(x, "numel") else x.size) // n
         shp = tuple(x.shape[:-1]) + (nb,)
-        inter = self.s.cfg.layout == L_INTERLEAVED
+        inter = self._inter
         if out_re is None:
             out_re = _empty_like_batch(x, shp + (2,) if inter else shp)
             out_im = None if inter else _empty_like_batch(x, shp)
@@ -413,7 +412,7 @@ class Transform:
 
     def c2r(self, Xr, Xi=None, out=None):
         n, nb = self.n, self.n // 2 + 1
-        inter = self.s.cfg.layout == L_INTERLEAVED
+        inter = self._inter
         cnt = Xr.numel() if hasattr(Xr, "numel") else Xr.size
         batch = cnt // (2 * nb if inter else nb)
         shp = (tuple(Xr.shape[:-2]) if inter else tuple(Xr.shape[:-1])) + (n,)
