@@ -481,10 +481,17 @@ static bool build_tc_tables(DevicePlan* p, std::string& err) {
     return true;
 }
 
+// FAF_CUDA_FOURSTEP_16K=1: C2C of 16384 points (without the tensor-core
+// form) on the multi-CTA two-pass four-step (128 x 128) instead of one CTA.
+static bool fourstep_16k(int n, uint32_t flags) {
+    const char* env = std::getenv("FAF_CUDA_FOURSTEP_16K");
+    return n == 16384 && !(flags & FAF_FLAG_TENSOR_CORE) && env && env[0] == '1';
+}
+
 DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::string& err) {
     DevicePlan* p = nullptr;
     if (is_7_smooth(n)) {
-        if (needs_four_step(n)) {
+        if (needs_four_step(n) || fourstep_16k(n, flags)) {
             p = new_plan(Kind::C2C_LARGE, n);
             if (!build_large(p, n, err)) { plan_free(p); return nullptr; }
             p->inverse = inverse;

@@ -163,7 +163,7 @@ cudaError_t prepare_pair() {
 
 template <int N1, int N2>
 cudaError_t launch_pair(const Large2Args& a, cudaStream_t st) {
-    static_assert(N1 * N2 > 16384 && N2 % Cols<N1>::W == 0 && N1 % Cols<N2>::W == 0,
+    static_assert(N1 * N2 >= 16384 && N2 % Cols<N1>::W == 0 && N1 % Cols<N2>::W == 0,
                   "column / row blocks must tile the transform");
     constexpr size_t sm1 = Cols<N1>::smem(), sm2 = Cols<N2>::smem();
     cudaError_t e = prepare_pair<N1, N2>();
@@ -191,7 +191,7 @@ cudaError_t launch_pair(const Large2Args& a, cudaStream_t st) {
 }  // namespace l2p
 
 bool large_pot2_supported(int n1, int n2) {
-    return (n1 == 128 && n2 == 256) || (n1 == 256 && n2 == 256);
+    return (n1 == 128 && n2 == 128) || (n1 == 128 && n2 == 256) || (n1 == 256 && n2 == 256);
 }
 
 long long large_pot2_chunk(long long n) {
@@ -204,6 +204,7 @@ int large_pot2_launches(int n1, int n2, long long batch) {
 }
 
 cudaError_t large_pot2_prepare(int n1, int n2) {
+    if (n1 == 128 && n2 == 128) return l2p::prepare_pair<128, 128>();
     if (n1 == 128 && n2 == 256) return l2p::prepare_pair<128, 256>();
     if (n1 == 256 && n2 == 256) return l2p::prepare_pair<256, 256>();
     return cudaErrorInvalidValue;
@@ -211,6 +212,7 @@ cudaError_t large_pot2_prepare(int n1, int n2) {
 
 cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st) {
     if (a.batch <= 0) return cudaSuccess;
+    if (n1 == 128 && n2 == 128) return l2p::launch_pair<128, 128>(a, st);
     if (n1 == 128 && n2 == 256) return l2p::launch_pair<128, 256>(a, st);
     if (n1 == 256 && n2 == 256) return l2p::launch_pair<256, 256>(a, st);
     return cudaErrorInvalidValue;

@@ -446,3 +446,21 @@ def test_host_buffers_on_four_step_and_host_mask(cuda):
     xs = rng.standard_normal((5, 4096)).astype(np.float32)
     y = p.pipeline(xs)
     assert orc.rel_l2(y, orc.pipeline(xs, [(orc.OP_MUL, 0, 0)], m, np.zeros_like(m))) <= REL_L2_TOL
+
+
+@pytest.mark.parametrize("inverse", [False, True])
+def test_c2c_16384_two_pass_four_step(cuda, monkeypatch, inverse):
+    """FAF_CUDA_FOURSTEP_16K=1 runs the 16384-point C2C as the multi-CTA
+    128 x 128 two-pass four-step instead of one CTA per transform."""
+    import fastandfourier_b200 as F
+    monkeypatch.setenv("FAF_CUDA_FOURSTEP_16K", "1")
+    torch = cuda
+    n = 16384
+    rng = seeded(161 + inverse)
+    re = rng.uniform(-1, 1, (5, n)).astype(np.float32)
+    im = rng.uniform(-1, 1, (5, n)).astype(np.float32)
+    t = F.Transform.fft(n, inverse=inverse)
+    assert t.kind == "c2c-4step"
+    yr, yi = t.c2c(dev(torch, re), dev(torch, im))
+    want = orc.fp64_c2c(re, im, inverse=inverse)
+    assert orc.rel_l2_complex(host(yr), host(yi), want) <= REL_L2_TOL
