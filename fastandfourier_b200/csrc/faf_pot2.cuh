@@ -320,19 +320,54 @@ __device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
         const int j = Dft<R>::slot(r);
         return cf{xr[h][j], xi[h][j]};
     };
-    if (t != 0) {
+    // Other threads: bins k1 = t + i NB and N - k1 (butterflies t and NB - t).
+    // Thread 0: butterfly NB / 2 pairs with itself, and so does butterfly 0.
+    if constexpr (Pl::T > 32) {
+        // several warps per transform: only one of them splits on thread 0,
+        // and separate branches cost fewer registers than selects
+        if (t != 0) {
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-            const int k1 = b[0] + r * NB, k2 = N - k1;
-            if (k1 < k2) pair(k1, Z(0, r), Z(1, R - 1 - r));
-            else pair(k2, Z(1, R - 1 - r), Z(0, r));
+            for (int r = 0; r < R; r++) {
+                const int k1 = b[0] + r * NB, k2 = N - k1;
+                if (k1 < k2) pair(k1, Z(0, r), Z(1, R - 1 - r));
+                else pair(k2, Z(1, R - 1 - r), Z(0, r));
+            }
+        } else {
+            dc(Z(0, 0));
+#pragma unroll
+            for (int r = 1; r <= R / 2; r++) pair(r * NB, Z(0, r), Z(0, R - r));
+#pragma unroll
+            for (int r = 0; r < R / 2; r++) pair(NB / 2 + r * NB, Z(1, r), Z(1, R - 1 - r));
         }
-    } else {
-        dc(Z(0, 0));
+        return;
+    }
+    // one warp (or less) per transform: every warp holds a thread 0, so one
+    // call sequence for all threads, thread 0 swapping in its pairs by selects
+    // (for i < R / 2 from butterfly NB / 2, after that from butterfly 0)
+    const bool t0 = t == 0;
+    if (t0) dc(Z(0, 0));
 #pragma unroll
-        for (int r = 1; r <= R / 2; r++) pair(r * NB, Z(0, r), Z(0, R - r));
-#pragma unroll
-        for (int r = 0; r < R / 2; r++) pair(NB / 2 + r * NB, Z(1, r), Z(1, R - 1 - r));
+    for (int i = 0; i < R; i++) {
+        const int k1 = b[0] + i * NB, k2 = N - k1;
+        const bool lo = k1 < k2;
+        int k = lo ? k1 : k2;
+        cf za = lo ? Z(0, i) : Z(1, R - 1 - i);
+        cf zb = lo ? Z(1, R - 1 - i) : Z(0, i);
+        if (i < R / 2) {
+            if (t0) {
+                k = NB / 2 + i * NB;
+                za = Z(1, i);
+                zb = Z(1, R - 1 - i);
+            }
+        } else {
+            const int j = i - R / 2 + 1;
+            if (t0) {
+                k = j * NB;
+                za = Z(0, j);
+                zb = Z(0, R - j);
+            }
+        }
+        pair(k, za, zb);
     }
 }
 
