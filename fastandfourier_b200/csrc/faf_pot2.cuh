@@ -286,7 +286,9 @@ struct LastPairs {
     static constexpr bool ok = Pl::NS >= 2 && R == 8;
 };
 
-template <int N, bool TWS_SMEM, int ORD = 0, class Dc, class Pair>
+// SEL: 1 makes thread 0 swap its pairs in by selects (no branch), 0 gives it
+// a branch of its own, -1 picks selects for one-warp transforms only.
+template <int N, bool TWS_SMEM, int ORD = 0, int SEL = -1, class Dc, class Pair>
 __device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
                                               const float2* __restrict__ tws, const Dc& dc,
                                               const Pair& pair) {
@@ -322,7 +324,7 @@ __device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
     };
     // Other threads: bins k1 = t + i NB and N - k1 (butterflies t and NB - t).
     // Thread 0: butterfly NB / 2 pairs with itself, and so does butterfly 0.
-    if constexpr (Pl::T > 32) {
+    if constexpr (SEL == 0 || (SEL < 0 && Pl::T > 32)) {
         // several warps per transform: only one of them splits on thread 0,
         // and separate branches cost fewer registers than selects
         if (t != 0) {

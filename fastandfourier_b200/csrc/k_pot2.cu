@@ -111,6 +111,14 @@ __device__ __forceinline__ void ct_r2c_post(int t, const SmemC& mid,
     }
 }
 
+// Thread 0's bin pairs in the fused R2C post-pass: by selects (no branch
+// splitting its warp) for the ring kernel of inner length 2048, where they
+// cost no spills and took the n = 4096 R2C from 4641 to 5000 GB/s on B200;
+// elsewhere the default (selects only for one-warp transforms), because the
+// selects spill at other lengths and in the direct-load kernels.
+template <int N, bool RING>
+constexpr int kR2cSel = (RING && N == 2048) ? 1 : -1;
+
 // RING: inputs land in the CTA's ring by bulk copy (in_a 16-byte aligned,
 // in_dist a multiple of 4); otherwise the first stage loads them.
 template <int N, bool RING>
@@ -160,7 +168,7 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
                 // one branch per transform on the layout: a per-store branch
                 // costs the fused stage registers it does not have
                 auto post = [&](const auto& out) {
-                    fafct::ct_last_pairs<N, kTw<N, kRO>, kRO>(
+                    fafct::ct_last_pairs<N, kTw<N, kRO>, kRO, kR2cSel<N, RING>>(
                         q.t, q.ws, q.tw,
                         [&](cf z) {
                             out.put(0, (z.x + z.y) * sc, 0.f);
