@@ -111,11 +111,13 @@ __device__ __forceinline__ void ct_r2c_post(int t, const SmemC& mid,
     }
 }
 
-// Thread 0's bin pairs in the fused R2C post-pass: by selects (no branch
-// splitting its warp) for the ring kernel of inner length 2048, where they
-// cost no spills and took the n = 4096 R2C from 4641 to 5000 GB/s on B200;
-// elsewhere the default (selects only for one-warp transforms), because the
-// selects spill at other lengths and in the direct-load kernels.
+// Thread 0's bin pairs in the fused R2C post-pass and in the pipeline's
+// single-MUL middle: by selects (no branch splitting its warp) for the ring
+// kernels of inner length 2048, measured on B200: the n = 4096 R2C went from
+// 4641 to 5007 GB/s (no spills), the pipeline from 2369 to 2432 GB/s (despite
+// 40 bytes of spills).  Elsewhere the default (selects only for one-warp
+// transforms): the selects spill more at other lengths and in the direct-load
+// kernels.
 template <int N, bool RING>
 constexpr int kR2cSel = (RING && N == 2048) ? 1 : -1;
 
@@ -453,11 +455,11 @@ __device__ __forceinline__ void pipe_middle(int t, const SmemC& mid,
 // The same bin-pair pass fused with the forward transform's last stage
 // (fafct::ct_last_pairs): each thread transforms the bins it owns in
 // registers and writes the pre-pass result back to those same slots.
-template <int N, class Ops>
+template <int N, int SEL = -1, class Ops>
 __device__ __forceinline__ void pipe_middle_fused(int t, float2* ws, const float2* tw,
                                                   const float2* __restrict__ stw, const Ops& ops) {
     const SmemC mid{ws};
-    fafct::ct_last_pairs<N, kTw<N, kRO>, kRO>(
+    fafct::ct_last_pairs<N, kTw<N, kRO>, kRO, SEL>(
         t, ws, tw,
         [&](cf z) {
             const cf x0 = ops(0, cf{z.x + z.y, 0.f});
@@ -517,7 +519,7 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
                     q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, q.sync);
             }
             if (ops_single_mul(a))
-                pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsMul1{&a.ops[0]});
+                pipe_middle_fused<N, kR2cSel<N, RING>>(q.t, q.ws, q.tw, a.stw, OpsMul1{&a.ops[0]});
             else
                 pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsAny{&a});
         } else {
