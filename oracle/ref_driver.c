@@ -15,6 +15,12 @@
  * twiddles[1] as recursion work), so every worker thread creates its own
  * transform objects and runs a contiguous slice of the batch through the
  * reference's public faf_execute (include/fastandfourier.h:950).
+ *
+ * Timing follows the reference's own benchmarks (plan once, execute in a
+ * loop: benchmarks/benchmark_throughput.cpp:34-39): a session
+ * (refdrv_open_*) starts its worker threads, creates their transforms and
+ * runs one warm-up execute on each, and refdrv_session_run then times
+ * nothing but faf_execute calls.
  */
 #define _GNU_SOURCE
 #include <pthread.h>
@@ -96,22 +102,45 @@ static faf_transform *make_transform(const job *j) {
     return NULL;
 }
 
-static void *run_job(void *arg) {
-    job *j = (job *)arg;
-    j->rc = 0;
-    if (j->b0 >= j->b1) return NULL;
-    faf_transform *t = make_transform(j);
-    if (!t) { drv_fail("create"); j->rc = -1; return NULL; }
-    size_t n = j->n, nb = n / 2 + 1;
-    float *frame = NULL;
-    float *win = NULL;
+/* Per-thread state of a session: the thread's own transform and, for the
+ * STFT, its frame and window buffers. */
+typedef struct {
+    faf_transform *t;
+    float *frame, *win;
+} worker_state;
+
+/* Creation is serialised: chirp_compile reads the reference's global,
+ * unlocked registry (src/chirp.c:39-41). */
+static pthread_mutex_t g_create_mu = PTHREAD_MUTEX_INITIALIZER;
+
+static int worker_setup(const job *j, worker_state *w) {
+    memset(w, 0, sizeof(*w));
+    pthread_mutex_lock(&g_create_mu);
+    w->t = make_transform(j);
+    pthread_mutex_unlock(&g_create_mu);
+    if (!w->t) { drv_fail("create"); return -1; }
     if (j->kind == JOB_STFT) {
-        frame = (float *)calloc(n, sizeof(float));
-        win = (float *)calloc(j->win, sizeof(float));
-        if (!frame || !win) { j->rc = -1; goto done; }
+        w->frame = (float *)calloc(j->n, sizeof(float));
+        w->win = (float *)calloc(j->win, sizeof(float));
+        if (!w->frame || !w->win) return -1;
         /* Reference symmetric Hann, src/faf_twiddles.c:159-163. */
-        faf_gen_hann_window_f32(win, j->win);
+        faf_gen_hann_window_f32(w->win, j->win);
     }
+    return 0;
+}
+
+static void worker_teardown(worker_state *w) {
+    free(w->frame);
+    free(w->win);
+    if (w->t) faf_destroy_transform(w->t);
+    memset(w, 0, sizeof(*w));
+}
+
+/* Run transforms [j->b0, j->b1) of the job's buffers through the worker's
+ * transform with the reference's public faf_execute. */
+static int worker_slice(const job *j, worker_state *w) {
+    faf_transform *t = w->t;
+    size_t n = j->n, nb = n / 2 + 1;
     for (size_t b = j->b0; b < j->b1; b++) {
         faf_buffer in, out;
         int rc = 0;
@@ -149,50 +178,249 @@ static void *run_job(void *arg) {
             rc = faf_execute(t, &out, &in);
             break;
         case JOB_STFT: {
-            /* Signal b, frame f: x[b*L + f*hop + i] * w[i] for i < win,
-             * zero-padded to n, then the reference R2C of n. */
+            /* Signal b / frames, frame b % frames: x[sig*L + f*hop + i] * w[i]
+             * for i < win, zero-padded to n, then the reference R2C of n. */
             size_t sig = b / j->frames, f = b % j->frames;
             const float *x = j->in_re + sig * j->sig_len + f * j->hop;
-            for (size_t i = 0; i < j->win; i++) frame[i] = x[i] * win[i];
-            in = faf_buffer_real(frame, n);
+            for (size_t i = 0; i < j->win; i++) w->frame[i] = x[i] * w->win[i];
+            in = faf_buffer_real(w->frame, n);
             out = faf_buffer_hermitian(j->out_re + b * nb, j->out_im + b * nb, nb);
             rc = faf_execute(t, &out, &in);
             break;
         }
         }
-        if (rc != 0) { drv_fail("execute"); j->rc = -1; break; }
+        if (rc != 0) { drv_fail("execute"); return -1; }
     }
-done:
-    free(frame);
-    free(win);
-    faf_destroy_transform(t);
+    return 0;
+}
+
+/* One transform of zeros through the worker's transform, so one-time work
+ * that the reference does on the first execute (the pipeline JIT compiles
+ * its trampoline with gcc then, src/jit/faf_jit.c:1156-1202) happens before
+ * any timed run. */
+static int worker_warm(const job *proto, worker_state *w) {
+    size_t n = proto->n, nb = n / 2 + 1, el = proto->f64 ? 2 : 1;
+    size_t in_len = n, out_len = n;
+    switch (proto->kind) {
+    case JOB_C2C: in_len = out_len = n * el; break;
+    case JOB_R2C: out_len = nb; break;
+    case JOB_C2R: in_len = nb; break;
+    case JOB_PIPE: break;
+    case JOB_CWT: out_len = proto->rows * n; break;
+    case JOB_ICWT: in_len = proto->rows * n; break;
+    case JOB_STFT: in_len = proto->win; out_len = nb; break;
+    }
+    float *a = (float *)calloc(2 * in_len + 2 * out_len, sizeof(float));
+    if (!a) return -1;
+    job j = *proto;
+    j.in_re = a; j.in_im = a + in_len;
+    j.out_re = a + 2 * in_len; j.out_im = a + 2 * in_len + out_len;
+    j.b0 = 0; j.b1 = 1;
+    if (j.kind == JOB_STFT) { j.frames = 1; j.sig_len = j.win; }
+    int rc = worker_slice(&j, w);
+    free(a);
+    return rc;
+}
+
+/*
+ * A session: `nthreads` persistent worker threads, each holding its own
+ * transform (the reference's transforms are not re-entrant), created and
+ * warmed once when the session opens.  refdrv_session_run() hands every
+ * worker a contiguous slice of the batch and waits for all of them, so a
+ * timed run contains faf_execute calls and nothing else: no thread start,
+ * no create, no JIT compile.
+ */
+typedef struct refdrv_session {
+    job proto;
+    int nthreads;
+    pthread_t *th;
+    job *jobs;
+    worker_state *ws;
+    pthread_mutex_t mu;
+    pthread_cond_t go, done;
+    unsigned long gen;   /* incremented per run (and once to quit) */
+    int pending;         /* workers still running the current generation */
+    int quit;
+    int ready;           /* workers that finished setup */
+    int setup_failed;
+} refdrv_session;
+
+typedef struct { refdrv_session *s; int id; } worker_arg;
+
+static void *worker_main(void *arg) {
+    worker_arg *wa = (worker_arg *)arg;
+    refdrv_session *s = wa->s;
+    const int id = wa->id;
+    free(wa);
+    int rc = worker_setup(&s->proto, &s->ws[id]);
+    if (rc == 0) rc = worker_warm(&s->proto, &s->ws[id]);
+    pthread_mutex_lock(&s->mu);
+    if (rc != 0) s->setup_failed = 1;
+    s->ready++;
+    pthread_cond_broadcast(&s->done);
+    unsigned long seen = 0;
+    for (;;) {
+        while (s->gen == seen) pthread_cond_wait(&s->go, &s->mu);
+        seen = s->gen;
+        if (s->quit) break;
+        pthread_mutex_unlock(&s->mu);
+        job *j = &s->jobs[id];
+        j->rc = (j->b0 < j->b1) ? worker_slice(j, &s->ws[id]) : 0;
+        pthread_mutex_lock(&s->mu);
+        if (--s->pending == 0) pthread_cond_broadcast(&s->done);
+    }
+    pthread_mutex_unlock(&s->mu);
+    worker_teardown(&s->ws[id]);
     return NULL;
 }
 
-static int run_batched(const job *proto, size_t batch, int nthreads) {
+void refdrv_session_close(refdrv_session *s);
+
+static refdrv_session *session_open(const job *proto, int nthreads) {
     if (nthreads < 1) nthreads = 1;
-    if ((size_t)nthreads > batch) nthreads = (int)(batch ? batch : 1);
-    job *jobs = (job *)calloc((size_t)nthreads, sizeof(job));
-    pthread_t *th = (pthread_t *)calloc((size_t)nthreads, sizeof(pthread_t));
-    if (!jobs || !th) { free(jobs); free(th); return -1; }
-    size_t per = batch / (size_t)nthreads, rem = batch % (size_t)nthreads, at = 0;
+    refdrv_session *s = (refdrv_session *)calloc(1, sizeof(*s));
+    if (!s) return NULL;
+    s->proto = *proto;
+    s->nthreads = nthreads;
+    s->th = (pthread_t *)calloc((size_t)nthreads, sizeof(pthread_t));
+    s->jobs = (job *)calloc((size_t)nthreads, sizeof(job));
+    s->ws = (worker_state *)calloc((size_t)nthreads, sizeof(worker_state));
+    pthread_mutex_init(&s->mu, NULL);
+    pthread_cond_init(&s->go, NULL);
+    pthread_cond_init(&s->done, NULL);
+    if (!s->th || !s->jobs || !s->ws) { free(s->th); free(s->jobs); free(s->ws); free(s); return NULL; }
+    int started = 0;
     for (int i = 0; i < nthreads; i++) {
-        jobs[i] = *proto;
-        jobs[i].b0 = at;
-        at += per + ((size_t)i < rem ? 1 : 0);
-        jobs[i].b1 = at;
+        worker_arg *wa = (worker_arg *)malloc(sizeof(worker_arg));
+        if (!wa) break;
+        wa->s = s; wa->id = i;
+        if (pthread_create(&s->th[i], NULL, worker_main, wa) != 0) { free(wa); break; }
+        started++;
     }
+    pthread_mutex_lock(&s->mu);
+    while (s->ready < started) pthread_cond_wait(&s->done, &s->mu);
+    const int failed = s->setup_failed || started < nthreads;
+    pthread_mutex_unlock(&s->mu);
+    s->nthreads = started;
+    if (failed) { refdrv_session_close(s); return NULL; }
+    return s;
+}
+
+/* Run `batch` transforms of the given buffers (layout as for the one-shot
+ * calls below) on the session's workers; 0 on success. */
+int refdrv_session_run(refdrv_session *s, size_t batch, const void *in_re, const void *in_im,
+                       void *out_re, void *out_im) {
+    if (!s) return -1;
+    const size_t nth = (size_t)s->nthreads;
+    size_t per = batch / nth, rem = batch % nth, at = 0;
+    pthread_mutex_lock(&s->mu);
+    for (size_t i = 0; i < nth; i++) {
+        job *j = &s->jobs[i];
+        *j = s->proto;
+        j->in_re = (const float *)in_re; j->in_im = (const float *)in_im;
+        j->out_re = (float *)out_re; j->out_im = (float *)out_im;
+        j->b0 = at;
+        at += per + (i < rem ? 1 : 0);
+        j->b1 = at;
+        j->rc = 0;
+    }
+    s->pending = s->nthreads;
+    s->gen++;
+    pthread_cond_broadcast(&s->go);
+    while (s->pending > 0) pthread_cond_wait(&s->done, &s->mu);
+    pthread_mutex_unlock(&s->mu);
     int rc = 0;
-    if (nthreads == 1) {
-        run_job(&jobs[0]);
-    } else {
-        for (int i = 0; i < nthreads; i++) pthread_create(&th[i], NULL, run_job, &jobs[i]);
-        for (int i = 0; i < nthreads; i++) pthread_join(th[i], NULL);
-    }
-    for (int i = 0; i < nthreads; i++) if (jobs[i].rc != 0) rc = -1;
-    free(jobs);
-    free(th);
+    for (size_t i = 0; i < nth; i++) if (s->jobs[i].rc != 0) rc = -1;
     return rc;
+}
+
+int refdrv_session_threads(const refdrv_session *s) { return s ? s->nthreads : 0; }
+
+void refdrv_session_close(refdrv_session *s) {
+    if (!s) return;
+    pthread_mutex_lock(&s->mu);
+    s->quit = 1;
+    s->gen++;
+    pthread_cond_broadcast(&s->go);
+    pthread_mutex_unlock(&s->mu);
+    for (int i = 0; i < s->nthreads; i++) pthread_join(s->th[i], NULL);
+    pthread_mutex_destroy(&s->mu);
+    pthread_cond_destroy(&s->go);
+    pthread_cond_destroy(&s->done);
+    free(s->th);
+    free(s->jobs);
+    free(s->ws);
+    free(s);
+}
+
+static int run_batched(const job *proto, size_t batch, int nthreads) {
+    if ((size_t)nthreads > batch) nthreads = (int)(batch ? batch : 1);
+    refdrv_session *s = session_open(proto, nthreads);
+    if (!s) return -1;
+    int rc = refdrv_session_run(s, batch, proto->in_re, proto->in_im, proto->out_re, proto->out_im);
+    refdrv_session_close(s);
+    return rc;
+}
+
+/* Session constructors: the same parameters as the one-shot calls below,
+ * without the buffers and the batch. */
+refdrv_session *refdrv_open_c2c(size_t n, int inverse, int norm, uint32_t flags, int f64,
+                                int nthreads) {
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_C2C; j.n = n; j.inverse = inverse; j.norm = norm; j.flags = flags; j.f64 = f64;
+    return session_open(&j, nthreads);
+}
+
+refdrv_session *refdrv_open_r2c(size_t n, int norm, int nthreads) {
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_R2C; j.n = n; j.norm = norm;
+    return session_open(&j, nthreads);
+}
+
+refdrv_session *refdrv_open_pipeline(const char *src, size_t n, const float *h_re,
+                                     const float *h_im, size_t h_bins, int nthreads) {
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_PIPE; j.n = n; j.src = src;
+    j.h_re = h_re; j.h_im = h_im; j.h_bins = h_bins;
+    return session_open(&j, nthreads);
+}
+
+/* STFT sessions run batches counted in frames: batch = n_sig * frames. */
+refdrv_session *refdrv_open_stft(size_t n, size_t win, size_t hop, size_t sig_len,
+                                 int nthreads) {
+    if (win == 0 || win > n || hop == 0 || sig_len < win) {
+        snprintf(g_drv_err, sizeof(g_drv_err), "stft: bad framing");
+        return NULL;
+    }
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_STFT; j.n = n; j.norm = FAF_NORM_NONE;
+    j.win = win; j.hop = hop; j.sig_len = sig_len;
+    j.frames = 1 + (sig_len - win) / hop;
+    return session_open(&j, nthreads);
+}
+
+int refdrv_cwt_bank(size_t n, size_t *n_rows, size_t *n_bins, int *has_lowpass, float *psi);
+
+refdrv_session *refdrv_open_cwt(size_t n, int nthreads) {
+    size_t rows = 0;
+    if (refdrv_cwt_bank(n, &rows, NULL, NULL, NULL) != 0) return NULL;
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_CWT; j.n = n; j.rows = rows;
+    return session_open(&j, nthreads);
+}
+
+refdrv_session *refdrv_open_icwt(size_t n, int kind, int nthreads) {
+    size_t rows = 0;
+    if (refdrv_cwt_bank(n, &rows, NULL, NULL, NULL) != 0) return NULL;
+    job j;
+    memset(&j, 0, sizeof(j));
+    j.kind = JOB_ICWT; j.n = n; j.rows = rows; j.inverse = kind;
+    return session_open(&j, nthreads);
 }
 
 int refdrv_c2c(size_t n, int inverse, int norm, uint32_t flags, size_t batch,

@@ -16,7 +16,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _REF_DIR = os.path.join(_HERE, "_ref")
-REFERENCE_SRC = "/root/reference"
+# Where the reference's sources are (needed only to compile oracle/_ref;
+# the GPU host loads the prebuilt library).
+REFERENCE_SRC = os.environ.get("FAF_REFERENCE_SRC", "")
 _lib = None
 _isa = None
 _f32p = ctypes.POINTER(ctypes.c_float)
@@ -46,11 +48,17 @@ def available():
     return os.path.exists(lib_path())
 
 
+def sources_present():
+    return bool(REFERENCE_SRC) and os.path.isdir(os.path.join(REFERENCE_SRC, "src"))
+
+
 def build():
     """Compile the reference library from its sources (needs the sources)."""
-    if not os.path.isdir(REFERENCE_SRC):
-        raise RuntimeError("reference sources not present; the prebuilt library "
-                           "must travel with the repository")
+    if not REFERENCE_SRC:
+        raise RuntimeError("FAF_REFERENCE_SRC is not set: point it at the reference's source "
+                           "tree to compile oracle/_ref (the prebuilt library is used otherwise)")
+    if not sources_present():
+        raise RuntimeError(f"FAF_REFERENCE_SRC={REFERENCE_SRC!r} holds no reference sources")
     subprocess.run(["make", "-s", "-j8", "-C", _HERE, "ref", f"REF={REFERENCE_SRC}"],
                    check=True)
 
@@ -84,6 +92,18 @@ def lib():
         L.refdrv_recommended_size.argtypes = [i, sz]
         L.refdrv_recommended_size.restype = sz
         L.refdrv_try_create.argtypes = [i, sz, u32, i, ctypes.c_char_p, sz]
+        vp = ctypes.c_void_p
+        for name, args in (("refdrv_open_c2c", [sz, i, i, u32, i, i]),
+                           ("refdrv_open_r2c", [sz, i, i]),
+                           ("refdrv_open_pipeline", [ctypes.c_char_p, sz, _f32p, _f32p, sz, i]),
+                           ("refdrv_open_stft", [sz, sz, sz, sz, i]),
+                           ("refdrv_open_cwt", [sz, i]),
+                           ("refdrv_open_icwt", [sz, i, i])):
+            f = getattr(L, name)
+            f.argtypes, f.restype = args, vp
+        L.refdrv_session_run.argtypes = [vp, sz, vp, vp, vp, vp]
+        L.refdrv_session_threads.argtypes = [vp]
+        L.refdrv_session_close.argtypes = [vp]
         _lib = L
         _isa = isa()
     return _lib
@@ -214,3 +234,70 @@ def try_create(ttype, n, flags=0, layout=0):
     buf = ctypes.create_string_buffer(512)
     ok = lib().refdrv_try_create(ttype, n, flags, layout, buf, 512)
     return bool(ok), buf.value.decode()
+
+
+class Session:
+    """Persistent reference workers for timing: `threads` threads, each with
+    its own transform, created and warmed (pipeline JIT compiled) when the
+    session opens.  run() executes a batch with nothing but faf_execute
+    calls, split into contiguous slices over the threads.
+
+    kind: "c2c", "c2c64", "r2c", "pipeline", "stft", "cwt", "icwt_dual".
+    """
+
+    def __init__(self, kind, n, threads=1, *, src=None, h=None, win=None, hop=None,
+                 sig_len=None, inverse=False, norm=1, flags=0):
+        L = lib()
+        self.kind, self.n = kind, n
+        self._keep = None
+        if kind in ("c2c", "c2c64"):
+            s = L.refdrv_open_c2c(n, int(inverse), norm, flags, int(kind == "c2c64"), threads)
+        elif kind == "r2c":
+            s = L.refdrv_open_r2c(n, norm, threads)
+        elif kind == "pipeline":
+            hr = hi = None
+            hb = 0
+            if h is not None:
+                self._keep = (_f32(h[0]), _f32(h[1]), src.encode())
+                hr, hi, hb = _p(self._keep[0]), _p(self._keep[1]), self._keep[0].size
+            else:
+                self._keep = (src.encode(),)
+            s = L.refdrv_open_pipeline(self._keep[-1], n, hr, hi, hb, threads)
+        elif kind == "stft":
+            self.frames = 1 + (sig_len - win) // hop
+            s = L.refdrv_open_stft(n, win, hop, sig_len, threads)
+        elif kind == "cwt":
+            s = L.refdrv_open_cwt(n, threads)
+        elif kind == "icwt_dual":
+            s = L.refdrv_open_icwt(n, 0, threads)
+        else:
+            raise ValueError(kind)
+        if not s:
+            raise RuntimeError("reference: " + L.refdrv_error().decode())
+        self._s = s
+        self.threads = L.refdrv_session_threads(s)
+
+    def run(self, batch, in_re, in_im=None, out_re=None, out_im=None):
+        """Execute `batch` transforms (STFT: signals) of C-contiguous arrays."""
+        if self.kind == "stft":
+            batch *= self.frames
+        ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
+        _check(lib().refdrv_session_run(self._s, batch, ptr(in_re), ptr(in_im), ptr(out_re),
+                                        ptr(out_im)))
+
+    def close(self):
+        if getattr(self, "_s", None):
+            lib().refdrv_session_close(self._s)
+            self._s = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,9 +1,10 @@
 #!/usr/bin/env python
 """Generate the golden fixtures from the reference library itself.
 
-Run in a container that has the reference sources at /root/reference:
+Run in a container that has the reference sources, with FAF_REFERENCE_SRC
+pointing at them:
 
-    python tests/golden/gen_golden.py
+    FAF_REFERENCE_SRC=<reference source tree> python tests/golden/gen_golden.py
 
 It builds the reference (oracle/Makefile `ref` target) if needed, runs every
 case of cases.py through the reference's public API (oracle/ref_driver.c ->
@@ -31,6 +32,8 @@ sys.path.insert(0, HERE)
 import cases  # noqa: E402
 from oracle import refimpl  # noqa: E402
 
+if not refimpl.sources_present():
+    sys.exit("gen_golden: set FAF_REFERENCE_SRC to the reference's source tree")
 REF_INCLUDE = os.path.join(refimpl.REFERENCE_SRC, "include")
 
 ABI_PROGRAM = r"""

@@ -53,7 +53,7 @@ def test_max_over_ranks_single_process():
 def test_reference_arm_rank0_only():
     sys.path.insert(0, ROOT)
     from oracle import refimpl
-    if not refimpl.available() and not os.path.isdir(refimpl.REFERENCE_SRC):
+    if not refimpl.available() and not refimpl.sources_present():
         pytest.skip("reference library not built")
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
