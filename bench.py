@@ -360,6 +360,74 @@ def max_over_ranks(x, dist, device):
     return float(t.item())
 
 
+def buffer_sets(workload, nbytes):
+    """Input/output buffer sets the timed loop rotates over: enough that
+    consecutive steps never share a set and the sets together exceed twice
+    the L2, so no step reads data the step before left in L2.  Working sets
+    under 16 MB (the launch-bound C2C of 256 x 1024) stay L2-resident: one."""
+    if nbytes < (16 << 20):
+        return 1
+    return max(2, -(-2 * L2_BYTES // nbytes))
+
+
+def fp64_check(workload, host_in, outs, batch, sample=8):
+    """rel L2 of the first and last `sample` transforms of a timed output
+    against FP64 numpy (the reference semantics: NumPy-style norm)."""
+    n = WORKLOADS[workload][1]
+    idx = sorted(set(list(range(min(sample, batch))) + list(range(max(0, batch - sample), batch))))
+    get = lambda a: a[idx].cpu().numpy().astype(np.float64)  # noqa: E731
+    if workload == "pipeline":
+        x = host_in[0][idx].astype(np.float64)
+        want = np.fft.irfft(np.fft.rfft(x, axis=-1) * notch_mask(n), n=n, axis=-1)
+        got = get(outs[0])
+    elif workload == "r2c":
+        want = np.fft.rfft(host_in[0][idx].astype(np.float64), axis=-1)
+        got = get(outs[0]) + 1j * get(outs[1])
+    elif workload.startswith("c2c"):
+        want = np.fft.fft(host_in[0][idx].astype(np.float64) + 1j * host_in[1][idx], axis=-1)
+        got = get(outs[0]) + 1j * get(outs[1])
+    else:
+        return None
+    return {"rel_l2_vs_fp64": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
+            "sample": f"transforms {idx[0]}..{idx[min(sample, len(idx)) - 1]} and the last "
+                      f"{min(sample, batch)} of the last timed step"}
+
+
+def time_steps(torch, stream, steps, fn):
+    """CUDA-event time of `steps` calls fn(i) on `stream` (ms per step)."""
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for i in range(steps):
+        fn(i)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / steps
+
+
+def r2c_subrecord(F, torch, stream, sets, host_in, steps, peak):
+    """Kernel-only R2C n=4096 on the headline's seed-1 signals (batch 8192),
+    rotating over the same input sets: the >= 70 % of HBM target's line."""
+    n, batch = 4096, WORKLOADS["r2c"][2]
+    t = F.Transform.rfft(n)
+    t.set_stream(stream)
+    outs = [alloc_outputs("r2c", batch, ins[0], torch) for ins, _ in sets]
+    step = lambda i: run_step(F, t, "r2c", sets[i % len(sets)][0], outs[i % len(sets)])  # noqa
+    for i in range(3):
+        step(i)
+    ms = time_steps(torch, stream, steps, step)
+    nbytes = algorithmic_bytes("r2c", batch)
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    chk = fp64_check("r2c", host_in, outs[(steps - 1) % len(sets)], batch)
+    rec = {"kernel": "k2_r2c", "workload": WORKLOADS["r2c"][0], "value": round(gbs, 1),
+           "unit": "GB/s", "ms_per_step": round(ms, 5), "frac": round(gbs / peak, 4),
+           "algorithmic_bytes_per_launch": nbytes, "traffic": ncu_traffic("r2c"),
+           "output_check": chk, "wait_status": t.wait_status(),
+           "gpu_launches": steps * F.lib().faf_cuda_last_launches()}
+    t.close()
+    return rec
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import fastandfourier_b200 as F
@@ -374,26 +442,38 @@ def run_ours(args, rank, world, local_rank):
     workload = args.workload
     desc, n, batch, _, flops_per = WORKLOADS[workload]
     host_in = make_inputs(workload, batch)
-    ins = [torch.from_numpy(a).cuda() for a in host_in]
-    outs = alloc_outputs(workload, batch, ins[0], torch)
-    t = build_transform(F, workload, torch)
-    stream = torch.cuda.current_stream()
-    t.set_stream(stream)
     nbytes = algorithmic_bytes(workload, batch)
+    nsets = buffer_sets(workload, nbytes)
+    sets = []
+    for _ in range(nsets):
+        ins = [torch.from_numpy(a).cuda() for a in host_in]
+        sets.append((ins, alloc_outputs(workload, batch, ins[0], torch)))
+    stream = torch.cuda.current_stream()
+    # the uneven plan replays a CUDA graph captured on fixed buffers: one plan
+    # per buffer set
+    plans = [build_transform(F, workload, torch)
+             for _ in range(nsets if workload == "uneven" else 1)]
+    for p in plans:
+        p.set_stream(stream)
+    t = plans[0]
 
-    for _ in range(max(args.warmup, 3)):
-        run_step(F, t, workload, ins, outs)
+    def step(i, plain=False, pl=None):
+        k = i % nsets
+        run_step(F, (pl or plans)[k % len(pl or plans)], workload, sets[k][0], sets[k][1],
+                 plain=plain)
+
+    for i in range(max(args.warmup, 3)):
+        step(i)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches = 0
     sampler = ClockSampler(local_rank)
     with sampler:
         ev0.record(stream)
-        for _ in range(args.steps):
-            run_step(F, t, workload, ins, outs)
+        for i in range(args.steps):
+            step(i)
         ev1.record(stream)
         torch.cuda.synchronize()
     # every step is the same call: the last one's launch count, times the steps
@@ -404,37 +484,31 @@ def run_ours(args, rank, world, local_rank):
     ms = max_over_ranks(ms, dist, "cuda")
     ms_per_step = ms / args.steps
     value = world * nbytes / (ms_per_step * 1e-3) / 1e9
+    last_outs = sets[(args.steps - 1) % nsets][1]
+    check = fp64_check(workload, host_in, last_outs, batch)
+    wait = t.wait_status() if hasattr(t, "wait_status") else None
     plain = None
     if workload == "uneven":
         # the plain GPU method on the same data: one batched launch per length
-        for _ in range(3):
-            run_step(F, t, workload, ins, outs, plain=True)
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            run_step(F, t, workload, ins, outs, plain=True)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        pms = ev0.elapsed_time(ev1) / args.steps
+        for i in range(3):
+            step(i, plain=True)
+        pms = time_steps(torch, stream, args.steps, lambda i: step(i, plain=True))
         plain = {"value": round(nbytes / (pms * 1e-3) / 1e9, 1), "ms_per_step": round(pms, 4),
                  "launches_per_step": len(set(uneven_lengths(batch))),
                  "speedup_of_persistent": round(pms / ms_per_step, 3)}
         # the tensor-core form of the same graph, with its error vs FP64
-        ttc = F.Uneven(uneven_lengths(batch), measure=True, tensor_core=True)
-        ttc.set_stream(stream)
-        for _ in range(3):
-            run_step(F, ttc, workload, ins, outs)
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            run_step(F, ttc, workload, ins, outs)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        tms = ev0.elapsed_time(ev1) / args.steps
+        ttc = [F.Uneven(uneven_lengths(batch), measure=True, tensor_core=True)
+               for _ in range(nsets)]
+        for p in ttc:
+            p.set_stream(stream)
+        for i in range(3):
+            step(i, pl=ttc)
+        tms = time_steps(torch, stream, args.steps, lambda i: step(i, pl=ttc))
         ls = uneven_lengths(batch)
         offs = np.concatenate([[0], np.cumsum(ls)])
         errs = []
-        yr, yi = outs[0].cpu().numpy(), outs[1].cpu().numpy()
+        o = sets[(args.steps - 1) % nsets][1]
+        yr, yi = o[0].cpu().numpy(), o[1].cpu().numpy()
         for j in range(0, len(ls), max(1, len(ls) // 16)):  # every size class
             a, b = offs[j], offs[j + 1]
             want = np.fft.fft(host_in[0][a:b].astype(np.float64) + 1j * host_in[1][a:b])
@@ -445,33 +519,30 @@ def run_ours(args, rank, world, local_rank):
                                      "speedup_over_plain": round(pms / tms, 3),
                                      "max_rel_l2_vs_fp64": max(errs),
                                      "sample": f"{len(errs)} transforms across the lengths"}
-        ttc.close()
+        for p in ttc:
+            p.close()
 
     if workload == "c2c16384tc":
         # accuracy of the tensor-core form on a sample, and the plain CUDA-core
         # path on the same data
-        k = 4
-        want = np.fft.fft(host_in[0][:k].astype(np.float64) + 1j * host_in[1][:k], axis=-1)
-        got = outs[0][:k].cpu().numpy() + 1j * outs[1][:k].cpu().numpy()
-        acc = {"rel_l2_vs_fp64": float(np.linalg.norm(got - want) / np.linalg.norm(want)),
-               "sample": f"first {k} transforms", "tc_status": t.tc_status()}
+        acc = dict(check or {})
+        acc["tc_status"] = t.tc_status()
         tp = F.Transform.fft(n)
         tp.set_stream(stream)
-        for _ in range(3):
-            run_step(F, tp, workload, ins, outs)
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for _ in range(args.steps):
-            run_step(F, tp, workload, ins, outs)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        pms = ev0.elapsed_time(ev1) / args.steps
+        for i in range(3):
+            step(i, pl=[tp])
+        pms = time_steps(torch, stream, args.steps, lambda i: step(i, pl=[tp]))
         plain = {"value": round(nbytes / (pms * 1e-3) / 1e9, 1), "ms_per_step": round(pms, 4),
                  "speedup_of_tensor_core_form": round(pms / ms_per_step, 3)}
         # three radix-16 stages x (16384 / 16) / 128 tiles x six 128x32x16 MMAs
         tflops = batch * 3 * (16384 // 16 // 128) * 6 * 2 * 128 * 32 * 16 / (ms_per_step * 1e-3) / 1e12
         acc["tensor_tflops"] = round(tflops, 1)
         tp.close()
+
+    peak, peak_kind = measured_hbm_peak()
+    r2c = None
+    if workload == "pipeline" and not args.no_r2c:
+        r2c = r2c_subrecord(F, torch, stream, sets, host_in, args.steps, peak)
 
     # end to end through the public API with pinned host buffers
     host_pinned = [torch.from_numpy(a).pin_memory().numpy() for a in host_in]
@@ -490,14 +561,13 @@ def run_ours(args, rank, world, local_rank):
     d2h = sum(a.nbytes for a in host_out)
     e2e_value = world * nbytes / e2e_s / 1e9
 
-    peak, peak_kind = measured_hbm_peak()
     achieved = nbytes / (ms_per_step * 1e-3) / 1e9
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
                 "traffic": ncu_traffic(workload),
                 "algorithmic_bytes_per_launch": nbytes,
                 "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
-                           "uneven": "k_uneven_large", "c2c16384tc": "k2_c2c_tc",
+                           "uneven": "k_large_pot2 (the 65536-point class)", "c2c16384tc": "k2_c2c_tc",
                            "c2c4096fp64": "k64_c2c", "istft": "k2_c2r + k_ola",
                            "cwt": "k2_c2r (bank rows) + k2_r2c",
                            "icwt": "k2_r2c (rows) + k_icwt_acc + k2_c2r"}.get(
@@ -523,8 +593,10 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic (seeded numpy PCG64)",
             "config": {"workload": desc, "n": n, "batch_per_gpu": batch,
                        "parallelism": f"replicas{world}",
-                       "l2": "inputs+outputs larger than L2 (no flush)"
-                       if nbytes > L2_BYTES else "L2-resident working set (launch-bound)"},
+                       "l2": (f"rotates over {nsets} input/output buffer sets of "
+                              f"{nbytes / 2**20:.0f} MiB (together > 2 x the 126 MB L2): no step "
+                              "reads data the previous step left in L2")
+                       if nsets > 1 else "L2-resident working set (launch-bound)"},
             "pct_hbm_peak": round(100 * achieved / peak, 2),
             "gflops_5nlog2n": round(world * batch * flops_per / (ms_per_step * 1e-3) / 1e9, 1)
             if flops_per else None,
@@ -535,14 +607,19 @@ def run_ours(args, rank, world, local_rank):
                     "api": "faf_execute_batched with pinned host buffers"},
             "gpu_launches": launches,
             "clocks": sampler.result(),
+            "output_check": check,
+            "wait_status": wait,
         }
+        if r2c is not None:
+            line["r2c"] = r2c
         if plain is not None and workload == "uneven":
             line["plain_one_launch_per_length"] = plain
         elif plain is not None:
             line["plain_cuda_core_path"] = plain
             line["accuracy"] = acc
         print(json.dumps(line), flush=True)
-    t.close()
+    for p in plans:
+        p.close()
     t_e2e.close()
     if dist:
         dist.barrier()
@@ -924,6 +1001,8 @@ def main():
     ap.add_argument("--workload", default="pipeline", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-r2c", action="store_true",
+                    help="skip the R2C kernel-only sub-record of the pipeline line")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))

@@ -9,6 +9,24 @@
 
 namespace fafk {
 
+// SM count of the current device, looked up once per device (a process may
+// drive several GPUs, and plans on each size their grids by its own count).
+inline int sm_count() {
+    constexpr int kMaxDev = 64;
+    static int cache[kMaxDev];  // 0: not looked up yet
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < kMaxDev && cache[dev] > 0) return cache[dev];
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms <= 0) {
+        cudaGetLastError();
+        sms = 1;
+    }
+    if (dev >= 0 && dev < kMaxDev) cache[dev] = sms;
+    return sms;
+}
+
 // Launch geometry chosen by the planner for one Shape.
 struct Geometry {
     int E;          // values per thread per stage (16 or 32)
@@ -124,6 +142,8 @@ struct LargeArgs {
     long long cta_floats;
 };
 // kind: 0 = C2C (C2CArgs), 1 = R2C, 2 = C2R, 3 = pipeline (RealArgs)
+// kernel attribute of the C2C four-step, and its module loaded on the current device
+cudaError_t large_c2c_prepare(const LargeArgs& a);
 cudaError_t launch_large(int kind, const LargeArgs& a, const void* args, long long batch,
                          int grid, cudaStream_t st);
 size_t large_smem(const LargeArgs& a, int threads);
@@ -176,7 +196,7 @@ struct Large2Args {
 bool large_pot2_supported(int n1, int n2);
 long long large_pot2_chunk(long long n);       // transforms per scratch chunk
 int large_pot2_launches(int n1, int n2, long long batch);
-cudaError_t large_pot2_prepare(int n1, int n2);  // kernel attributes, before any capture
+cudaError_t large_pot2_prepare(int n1, int n2);  // kernel attributes + module, before any capture
 cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st);
 
 // FP64 transforms (k_fp64.cu): kind 0 = C2C (C2C64Args), 1 = R2C, 2 = C2R

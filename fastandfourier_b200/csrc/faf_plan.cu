@@ -237,16 +237,7 @@ void free_size(FftSize& s) {
 // memory left after the workspaces holds up to `ring` input ring slots (n
 // float2 each, at most fafct::kRingMax) and `ring_extra` bytes behind them;
 // fewer than 2 slots means no ring.
-static int device_sms() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
-    return sms;
-}
+static int device_sms() { return fafk::sm_count(); }
 
 fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int ring,
                            int target_threads, size_t ring_extra, size_t slot_bytes) {
@@ -496,6 +487,10 @@ DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::stri
             if (!build_large(p, n, err)) { plan_free(p); return nullptr; }
             p->inverse = inverse;
             p->scale = scale;
+            // the allocation-free entry point's set-up (not needed by the
+            // regular path: a failure here only disables that entry point)
+            std::string why;
+            if (!noalloc_prepare(p, why)) cudaGetLastError();
             return p;
         }
         p = new_plan(Kind::C2C, n);
@@ -734,8 +729,9 @@ DevicePlan* plan_icwt_l1(int n, int rows, int lowpass, double dlog, double c, st
 
 // ---- four-step execution ---------------------------------------------------
 
-static fafk::LargeArgs large_args(DevicePlan* p) {
+fafk::LargeArgs large_args(const DevicePlan* p) {
     fafk::LargeArgs a;
+    std::memset(&a, 0, sizeof a);
     a.s1 = p->f1.shape(p->n1);
     a.s1.T = p->t1;
     a.s2 = p->f2.shape(p->n2);
@@ -752,13 +748,7 @@ static fafk::LargeArgs large_args(DevicePlan* p) {
 
 // One CTA per SM keeps the per-CTA scratch (2 or 4 x n floats) L2-resident.
 static int large_grid(long long batch) {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
+    const int sms = fafk::sm_count();
     return (int)std::max(1LL, std::min<long long>(batch, sms));
 }
 

@@ -165,6 +165,14 @@ int padded_threads(int m);
 bool needs_four_step(int n);
 // Power-of-two four-step plan that the multi-CTA two-pass kernels serve.
 bool large_pot2_plan(const DevicePlan* p);
+// Four-step arguments of plan p (scratch left NULL).
+fafk::LargeArgs large_args(const DevicePlan* p);
+// faf_noalloc.cu: on the plan's device (current), sets up everything
+// faf_cuda_execute_c2c_noalloc needs so that the call itself allocates
+// nothing -- the static scratch's device address and the kernels' modules,
+// both of which lazy module loading would otherwise bring in (allocating) at
+// the first call.  Called when a four-step C2C plan is created.
+bool noalloc_prepare(const DevicePlan* p, std::string& err);
 
 // Host FFT in double precision (table generation only).
 void host_dft_fp64(std::vector<double>& re, std::vector<double>& im);

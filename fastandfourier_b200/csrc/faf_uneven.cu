@@ -282,21 +282,6 @@ int sm_count() {
     return sms > 0 ? sms : 1;
 }
 
-fafk::LargeArgs large_args(const DevicePlan* L) {
-    fafk::LargeArgs la;
-    memset(&la, 0, sizeof la);
-    la.s1 = L->f1.shape(L->n1);
-    la.s1.T = L->t1;
-    la.s2 = L->f2.shape(L->n2);
-    la.s2.T = L->t2;
-    la.n1 = L->n1;
-    la.n2 = L->n2;
-    la.tw1 = L->f1.d_tw;
-    la.tw2 = L->f2.d_tw;
-    la.twn = L->d_tw_big;
-    return la;
-}
-
 // Build class descriptors, task lists and launch shapes for the current
 // tuning knobs.
 int build_schedule(faf_uneven* u) {

@@ -61,13 +61,7 @@ __global__ void __launch_bounds__(256) k_icwt_l1(const float* __restrict__ W, lo
 }
 
 unsigned grid_of(long long total) {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
+    const int sms = fafk::sm_count();
     const long long blocks = (total + 255) / 256;
     return (unsigned)std::max(1LL, std::min(blocks, (long long)sms * 8));
 }

@@ -40,6 +40,15 @@ size_t large_smem(const LargeArgs& a, int threads) {
     return (g1 > g2 ? g1 : g2) * sizeof(float);
 }
 
+cudaError_t large_c2c_prepare(const LargeArgs& a) {
+    cudaError_t e = prep(k4_c2c, large_smem(a, kLargeThreads));
+    if (e != cudaSuccess) return e;
+    // querying the kernel loads its module now (under lazy module loading it
+    // would otherwise load at the first launch)
+    cudaFuncAttributes fa;
+    return cudaFuncGetAttributes(&fa, k4_c2c);
+}
+
 cudaError_t launch_large(int kind, const LargeArgs& a, const void* args, long long batch,
                          int grid, cudaStream_t st) {
     if (batch <= 0) return cudaSuccess;

@@ -150,14 +150,24 @@ __global__ void __launch_bounds__(kThreads, 1)
 }
 
 // Kernel attributes (dynamic shared memory above 48 KB), set once per
-// process and before any stream capture reaches the launches.
+// device (prep memoises them) and before any stream capture reaches the
+// launches.
 template <int N1, int N2>
 cudaError_t prepare_pair() {
-    static cudaError_t done = cudaErrorNotReady;
-    if (done == cudaSuccess) return done;
     cudaError_t e = prep(k4p_col<N1, N2>, Cols<N1>::smem());
     if (e == cudaSuccess) e = prep(k4p_row<N1, N2>, Cols<N2>::smem());
-    done = e;
+    return e;
+}
+
+// The same, and the kernels' module loaded on the current device now rather
+// than at the first launch (lazy module loading): for callers that must not
+// allocate when they launch.
+template <int N1, int N2>
+cudaError_t load_pair() {
+    cudaError_t e = prepare_pair<N1, N2>();
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k4p_col<N1, N2>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k4p_row<N1, N2>);
     return e;
 }
 
@@ -168,13 +178,7 @@ cudaError_t launch_pair(const Large2Args& a, cudaStream_t st) {
     constexpr size_t sm1 = Cols<N1>::smem(), sm2 = Cols<N2>::smem();
     cudaError_t e = prepare_pair<N1, N2>();
     if (e != cudaSuccess) return e;
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
+    const int sms = fafk::sm_count();
     const long long chunk = std::max(1LL, a.scratch_transforms);
     for (long long b0 = 0; b0 < a.batch; b0 += chunk) {
         const long long nb = std::min(chunk, a.batch - b0);
@@ -204,9 +208,9 @@ int large_pot2_launches(int n1, int n2, long long batch) {
 }
 
 cudaError_t large_pot2_prepare(int n1, int n2) {
-    if (n1 == 128 && n2 == 128) return l2p::prepare_pair<128, 128>();
-    if (n1 == 128 && n2 == 256) return l2p::prepare_pair<128, 256>();
-    if (n1 == 256 && n2 == 256) return l2p::prepare_pair<256, 256>();
+    if (n1 == 128 && n2 == 128) return l2p::load_pair<128, 128>();
+    if (n1 == 128 && n2 == 256) return l2p::load_pair<128, 256>();
+    if (n1 == 256 && n2 == 256) return l2p::load_pair<256, 256>();
     return cudaErrorInvalidValue;
 }
 

@@ -551,13 +551,7 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
 
 template <class K>
 static unsigned persistent_grid(K kernel, const Geometry& g, long long batch) {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
+    const int sms = fafk::sm_count();
     const int per_sm = resident_ctas(kernel, g.threads, g.smem);
     const long long groups = (batch + g.G - 1) / g.G;
     const long long cap = (long long)sms * per_sm;

@@ -383,13 +383,7 @@ cudaError_t launch_n(const float2* tws, const C2CArgs& a, const void* gB, int* e
     constexpr size_t smem = smem_bytes<N>();
     cudaError_t e = prepare_n<N>();
     if (e != cudaSuccess) return e;
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 1;
-    }
+    const int sms = fafk::sm_count();
     constexpr int G = kThreads / P2<N>::T;
     const long long groups = (a.batch + G - 1) / G;
     const unsigned grid = (unsigned)std::max(1LL, std::min(groups, (long long)sms));

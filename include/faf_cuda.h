@@ -143,12 +143,17 @@ void faf_uneven_destroy(faf_uneven *u);
  * callers that must not allocate while they run: a real-time callback that
  * cannot wait inside the driver's allocator, or a program whose device memory
  * is fully reserved by another allocator so that a cudaMalloc would fail.
- * The four-step scratch is a fixed 16 MiB array per GPU, held from the
- * library's load until process exit; a length whose per-CTA scratch would
- * exceed it, host buffers and other plan kinds are rejected with an error.
- * All calls on a GPU share that array: launches that overlap on the GPU race
- * and must be serialised by the caller.  The first call on each device looks
- * up the array's device address and should come before any stream capture.
+ * The four-step scratch is a fixed 16 MiB array per GPU, held until process
+ * exit.  Creating a four-step C2C plan on a GPU places that array there (it
+ * loads the array's module, and the kernels' modules, which CUDA's default
+ * lazy module loading would otherwise do at the first call) and looks up its
+ * device address, so plan creation is where the allocation happens and the
+ * calls allocate nothing.  Power-of-two lengths run in chunks of
+ * 16 MiB / (8 n) transforms on the regular two-pass kernels; other lengths
+ * run one transform per CTA on at most 16 MiB / (8 n) CTAs.  A length whose
+ * per-transform scratch would exceed the array, host buffers and other plan
+ * kinds are rejected with an error.  All calls on a GPU share that array:
+ * launches that overlap on the GPU race and must be serialised by the caller.
  * Stream and synchronisation rules are those of faf_execute. */
 int faf_cuda_execute_c2c_noalloc(const faf_transform *t, float *out_re, float *out_im,
                                  const float *in_re, const float *in_im, size_t batch);

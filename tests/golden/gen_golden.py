@@ -32,8 +32,6 @@ sys.path.insert(0, HERE)
 import cases  # noqa: E402
 from oracle import refimpl  # noqa: E402
 
-if not refimpl.sources_present():
-    sys.exit("gen_golden: set FAF_REFERENCE_SRC to the reference's source tree")
 REF_INCLUDE = os.path.join(refimpl.REFERENCE_SRC, "include")
 
 ABI_PROGRAM = r"""
@@ -88,6 +86,8 @@ def abi_offsets(include_dir):
 
 
 def main():
+    if not refimpl.sources_present():
+        sys.exit("gen_golden: set FAF_REFERENCE_SRC to the reference's source tree")
     if not refimpl.available():
         refimpl.build()
     out = {}

@@ -24,16 +24,41 @@ def _ptr(t):
     return ctypes.c_void_p(t.data_ptr())
 
 
-@pytest.mark.parametrize("n,inverse", [(32768, False), (65536, False), (40000, True)])
-def test_noalloc_matches_regular_entry_point_twice(cuda, n, inverse):
+def test_noalloc_call_allocates_nothing(cuda):
+    """On a freshly created plan, the driver's free device memory is the same
+    before and after a call: creating the plan set up the static array and
+    loaded the kernels, so the call itself allocates nothing."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    L = F.lib()
+    n, batch = 65536, 3
+    rng = seeded(901)
+    re = torch.from_numpy(rng.uniform(-1, 1, (batch, n)).astype(np.float32)).cuda()
+    im = torch.from_numpy(rng.uniform(-1, 1, (batch, n)).astype(np.float32)).cuda()
+    out_r, out_i = torch.empty_like(re), torch.empty_like(im)
+    t = F.Transform.fft(n)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    rc = L.faf_cuda_execute_c2c_noalloc(t.ptr, _ptr(out_r), _ptr(out_i), _ptr(re), _ptr(im), batch)
+    assert rc == 0, F.C.error()
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    exact = orc.fp64_c2c(re.cpu().numpy(), im.cpu().numpy())
+    assert orc.rel_l2_complex(out_r.cpu().numpy(), out_i.cpu().numpy(), exact) <= REL_L2_TOL
+
+
+@pytest.mark.parametrize("n,inverse,batches", [
+    (32768, False, (5, 6)), (65536, False, (5, 6)), (40000, True, (5, 6)),
+    # past one chunk of the array: 64 transforms of 32768, 32 of 65536 fit
+    (32768, True, (70, 3)), (65536, False, (40, 33))])
+def test_noalloc_matches_regular_entry_point_twice(cuda, n, inverse, batches):
     import fastandfourier_b200 as F
     torch = cuda
     L = F.lib()
     t = F.Transform.fft(n, inverse=inverse)
     assert t.kind == "c2c-4step"
-    for call in range(2):
-        rng = seeded(500 + n + call)
-        batch = 5 + call
+    for call, batch in enumerate(batches):
+        rng = seeded(500 + n + call + batch)
         re = torch.from_numpy(rng.uniform(-1, 1, (batch, n)).astype(np.float32)).cuda()
         im = torch.from_numpy(rng.uniform(-1, 1, (batch, n)).astype(np.float32)).cuda()
         want_r, want_i = t.c2c(re, im)
