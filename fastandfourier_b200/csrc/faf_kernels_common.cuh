@@ -384,11 +384,12 @@ __device__ __forceinline__ cf mul_bin(const PipeOp& op, int k, cf v) {
 
 // Device spectral ops (chirp_register_spectral_device): gain, fixed phase,
 // and a circular delay whose phase is reduced in FP64 (k d mod n) before the
-// sine / cosine, so large k d keeps its accuracy.
-__device__ __forceinline__ cf delay_bin(const PipeOp& op, int k, cf v) {
-    const double r = fmod((double)k * op.d0, (double)op.n);
+// sine / cosine, so large k d keeps its accuracy.  The delay is out of line:
+// its FP64 code inlined at every bin of an unrolled pass bloats the kernel.
+static __device__ __noinline__ cf delay_bin(double d0, int n, int k, cf v) {
+    const double r = fmod((double)k * d0, (double)n);
     double s, c;
-    sincospi(-2.0 * r / (double)op.n, &s, &c);
+    sincospi(-2.0 * r / (double)n, &s, &c);
     const float fs = (float)s, fc = (float)c;
     return cf{v.x * fc - v.y * fs, fmaf(v.x, fs, v.y * fc)};
 }
@@ -399,16 +400,16 @@ __device__ __forceinline__ cf apply_op(const PipeOp& op, int k, cf v) {
     if (op.code == OP_BANDPASS && (k < op.lo || k > op.hi)) return cf{0.f, 0.f};
     if (op.code == OP_SCALE) return cf{v.x * op.f0, v.y * op.f0};
     if (op.code == OP_ROTATE) return cf{v.x * op.f0 - v.y * op.f1, fmaf(v.x, op.f1, v.y * op.f0)};
-    if (op.code == OP_DELAY) return delay_bin(op, k, v);
+    if (op.code == OP_DELAY) return delay_bin(op.d0, op.n, k, v);
     return v;
 }
 
-// Every op in order.  The loop bound is a compile-time constant and each op
-// is guarded (no early exit), so the loop unrolls with static accesses.
+// Every op in order, as a loop over the program (not unrolled): the passes
+// call this once per bin, and a copy of every op kind at each call site made
+// the generic-program kernels several times slower than the single-MUL one.
 __device__ __forceinline__ cf apply_pipe_ops(const RealArgs& a, int k, cf v) {
-#pragma unroll
-    for (int o = 0; o < kMaxOps; o++)
-        if (o < a.nops) v = apply_op(a.ops[o], k, v);
+#pragma unroll 1
+    for (int o = 0; o < a.nops; o++) v = apply_op(a.ops[o], k, v);
     return v;
 }
 
