@@ -350,7 +350,10 @@ extern "C" faf_transform* faf_create_fft(const faf_config* cfg) {
         fail("FP64 Bluestein transforms are not available on the CUDA backend");
         return nullptr;
     }
-    if (c.n > (size_t)fafp::kMaxLength) {
+    // the 2^16 cap on lengths; a Rader prime's inner length is p - 1, so
+    // 65537 (inner 65536) is within it
+    const bool rader = !bluestein && rader_eligible(c.n);
+    if (c.n > (size_t)fafp::kMaxLength && !(rader && c.n - 1 <= (size_t)fafp::kMaxLength)) {
         fail("FFT length %zu exceeds the 2^16 transform-length cap", c.n);
         return nullptr;
     }

@@ -499,6 +499,7 @@ int run_device(const faf_transform* t, DevicePlan* p, Request& r, cudaStream_t s
     case FAF_TRANSFORM_IFFT:
         e = fafp::exec_c2c(p, r.in_a, r.in_b, r.out_a, r.out_b, r.batch, in_dist, out_dist,
                            r.interleaved, nullptr, st);
+        launches = fafp::c2c_launches(p, r.batch);
         break;
     case FAF_TRANSFORM_RFFT:
         e = fafp::exec_r2c(p, r.in_a, r.out_a, r.out_b, r.batch, in_dist, out_dist,

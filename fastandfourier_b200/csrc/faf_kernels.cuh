@@ -113,6 +113,16 @@ __device__ __forceinline__ C2ROffsets c2r_offsets(const RealArgs& a, long long b
     return C2ROffsets{b * a.in_dist * fpe, b * a.out_dist, nullptr};
 }
 
+struct ConvArgs;
+// Rader / Bluestein whose inner length m needs the four-step (k_conv.cu):
+// the element-wise passes around the nested inner FFTs, over transforms
+// b0 .. b0 + nb - 1.  step 0: Rader gather into s; 1: Bluestein chirp into
+// s; 2: s *= B (dc[b] = s[b][0] first, when dc is set); 3: Rader scatter of
+// s (the unnormalised inverse FFT) and dc to the output; 4: Bluestein chirp
+// of s to the output.
+cudaError_t launch_conv_step(int step, const ConvArgs& a, long long b0, long long nb, int m,
+                             float* s_re, float* s_im, float2* dc, cudaStream_t st);
+
 struct ConvArgs {  // Rader (prime n) and Bluestein (any n)
     const float* in_re;
     const float* in_im;

@@ -328,6 +328,8 @@ static DevicePlan* new_plan(Kind k, int n) {
 
 void plan_free(DevicePlan* p) {
     if (!p) return;
+    plan_free(p->sub_fwd);
+    plan_free(p->sub_inv);
     free_size(p->inner);
     free_size(p->f1);
     free_size(p->f2);
@@ -479,6 +481,21 @@ static bool fourstep_16k(int n, uint32_t flags) {
     return n == 16384 && !(flags & FAF_FLAG_TENSOR_CORE) && env && env[0] == '1';
 }
 
+// Rader / Bluestein inner length m beyond one CTA: nested four-step plans,
+// forward and unnormalised inverse (the 1/m is applied by the last pass).
+static bool build_conv_inner(DevicePlan* p, int m, std::string& err) {
+    p->sub_fwd = plan_c2c(m, false, 1.0f, 0, err);
+    if (!p->sub_fwd) return false;
+    p->sub_inv = plan_c2c(m, true, 1.0f, 0, err);
+    if (!p->sub_inv) return false;
+    if (p->sub_fwd->kind != Kind::C2C_LARGE || p->sub_inv->kind != Kind::C2C_LARGE) {
+        err = "inner length " + std::to_string(m) + " is not a four-step length";
+        return false;
+    }
+    p->inner.n = m;
+    return true;
+}
+
 DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::string& err) {
     DevicePlan* p = nullptr;
     if (is_7_smooth(n)) {
@@ -503,12 +520,11 @@ DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::stri
     } else if (is_prime(n) && is_7_smooth(n - 1)) {
         // Rader: y = x0 + IDFT_m(DFT_m(x[g^j]) * DFT_m(W_p^{g^-j}))[...]
         const int m = n - 1;
-        if (m > kMaxSingleCta) {
-            err = "Rader prime " + std::to_string(n) + " exceeds the single-CTA inner length";
+        p = new_plan(Kind::RADER, n);
+        if (!(needs_four_step(m) ? build_conv_inner(p, m, err) : build_size(m, p->inner, err))) {
+            plan_free(p);
             return nullptr;
         }
-        p = new_plan(Kind::RADER, n);
-        if (!build_size(m, p->inner, err)) { plan_free(p); return nullptr; }
         const int g = primitive_root(n);
         const int ginv = (int)powmod(g, n - 2, n);
         std::vector<int> rin(m), rout(m);
@@ -538,13 +554,17 @@ DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::stri
         // Bluestein with M = next 5-smooth >= 2n - 1 (reference
         // src/faf_bluestein.c:19-22), chirp phi[k] = exp(-i pi k^2 / n).
         const long long M = next_5_smooth(2LL * n - 1);
-        if (M > kMaxSingleCta) {
+        if (M > 2LL * kMaxLength) {
             err = "Bluestein length " + std::to_string(n) + " (M = " + std::to_string(M) +
-                  ") exceeds the single-CTA inner length";
+                  ") exceeds the inner-length cap";
             return nullptr;
         }
         p = new_plan(Kind::BLUESTEIN, n);
-        if (!build_size((int)M, p->inner, err)) { plan_free(p); return nullptr; }
+        if (!(needs_four_step((int)M) ? build_conv_inner(p, (int)M, err)
+                                      : build_size((int)M, p->inner, err))) {
+            plan_free(p);
+            return nullptr;
+        }
         std::vector<float2> phi(n);
         std::vector<double> br(M, 0.0), bi(M, 0.0);
         for (int k = 0; k < n; k++) {
@@ -804,6 +824,70 @@ static cudaError_t run_large_pot2(DevicePlan* p, const float* in_re, const float
     return fafk::launch_large_pot2(p->n1, p->n2, a, st);
 }
 
+// Rader / Bluestein with nested four-step inner plans, in chunks of at most
+// 64 MB of scratch (two split-plane buffers): gather or chirp into S1, FFT
+// S1 -> S2, S2 *= B (Rader: DC sum kept), inverse FFT S2 -> S1, scatter or
+// chirp to the output (reference src/faf_fft_rader.c:136-232,
+// src/faf_bluestein.c:165-223, in the same order of operations).
+static long long conv_chunk(const DevicePlan* p, long long batch) {
+    const long long m = p->inner.n;
+    return std::max(1LL, std::min(batch, (64LL << 20) / (16 * m)));
+}
+
+static cudaError_t exec_conv_large(DevicePlan* p, const fafk::ConvArgs& a, cudaStream_t st) {
+    const int m = p->inner.n;
+    const long long chunk = conv_chunk(p, a.batch);
+    const size_t plane = (size_t)chunk * (size_t)m;
+    const size_t bytes = 4 * plane * sizeof(float) + (size_t)chunk * sizeof(float2);
+    {
+        std::lock_guard<std::mutex> lk(p->scratch_mu);
+        if (p->work_bytes < bytes) {
+            cudaFree(p->d_work);
+            p->d_work = nullptr;
+            p->work_bytes = 0;
+            cudaError_t e = cudaMalloc(&p->d_work, bytes);
+            if (e != cudaSuccess) return e;
+            p->work_bytes = bytes;
+        }
+    }
+    float* s1r = (float*)p->d_work;
+    float* s1i = s1r + plane;
+    float* s2r = s1i + plane;
+    float* s2i = s2r + plane;
+    float2* dc = (float2*)(s2i + plane);
+    const bool rader = p->kind == Kind::RADER;
+    cudaError_t e = cudaSuccess;
+    for (long long b0 = 0; b0 < a.batch && e == cudaSuccess; b0 += chunk) {
+        const long long nb = std::min(chunk, a.batch - b0);
+        e = fafk::launch_conv_step(rader ? 0 : 1, a, b0, nb, m, s1r, s1i, nullptr, st);
+        if (e == cudaSuccess)
+            e = exec_c2c(p->sub_fwd, s1r, s1i, s2r, s2i, nb, m, m, false, nullptr, st);
+        if (e == cudaSuccess)
+            e = fafk::launch_conv_step(2, a, b0, nb, m, s2r, s2i, rader ? dc : nullptr, st);
+        if (e == cudaSuccess)
+            e = exec_c2c(p->sub_inv, s2r, s2i, s1r, s1i, nb, m, m, false, nullptr, st);
+        if (e == cudaSuccess)
+            e = fafk::launch_conv_step(rader ? 3 : 4, a, b0, nb, m, s1r, s1i, dc, st);
+    }
+    return e;
+}
+
+int c2c_launches(const DevicePlan* p, long long batch) {
+    if (batch <= 0) return 0;
+    if (p->sub_fwd) {
+        const long long chunk = conv_chunk(p, batch);
+        long long k = 0;
+        for (long long b0 = 0; b0 < batch; b0 += chunk) {
+            const long long nb = std::min(chunk, batch - b0);
+            k += 3 + c2c_launches(p->sub_fwd, nb) + c2c_launches(p->sub_inv, nb);
+        }
+        return (int)k;
+    }
+    if (p->kind == Kind::C2C_LARGE && large_pot2_plan(p))
+        return fafk::large_pot2_launches(p->n1, p->n2, batch);
+    return 1;
+}
+
 bool large_pot2_plan(const DevicePlan* p) {
     return p->large && p->f1.ct_log2 && p->f2.ct_log2 && fafk::large_pot2_supported(p->n1, p->n2);
 }
@@ -842,11 +926,13 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
     }
     if (interleaved) return cudaErrorNotSupported;
     fafk::ConvArgs a;
+    std::memset(&a, 0, sizeof a);
     a.in_re = in_re; a.in_im = in_im; a.out_re = out_re; a.out_im = out_im;
     a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
     a.scale = p->scale; a.sgn = sgn; a.n = p->n;
     a.rin = p->d_rin; a.rout = p->d_rout; a.phi = p->d_phi; a.B = p->d_B;
     a.inv_inner = (float)(1.0 / (double)p->inner.n);
+    if (p->sub_fwd) return exec_conv_large(p, a, st);
     const int slots = p->inner.n;
     if (p->kind == Kind::RADER)
         return fafk::launch_rader(p->inner.shape(slots), geometry(p->inner, slots, 2, batch),

@@ -74,6 +74,10 @@ struct DevicePlan {
     FftSize f1, f2;
     int n1 = 0, n2 = 0, t1 = 0, t2 = 0;  // padded thread counts per sub-transform
     float2* d_tw_big = nullptr;  // four-step middle twiddles [k1 * n2 + c] = W_n^{c k1}
+    // Rader / Bluestein whose inner length needs the four-step: the inner
+    // FFT as nested four-step C2C plans, forward and unnormalised inverse
+    struct DevicePlan* sub_fwd = nullptr;
+    struct DevicePlan* sub_inv = nullptr;
     void* d_work = nullptr;      // per-CTA four-step scratch, grown on first use
     size_t work_bytes = 0;
     // tables
@@ -140,6 +144,8 @@ cudaError_t exec_r2c64(DevicePlan* p, const double* x, double* Xr, double* Xi, l
 cudaError_t exec_c2r64(DevicePlan* p, const double* Xr, const double* Xi, double* y,
                        long long batch, long long in_dist, long long out_dist, cudaStream_t st);
 void plan_free(DevicePlan* p);
+// Kernel launches of one exec_c2c of `batch` transforms of plan p.
+int c2c_launches(const DevicePlan* p, long long batch);
 
 // Device-pointer executes (enqueue on `st`).
 cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, float* out_re,
