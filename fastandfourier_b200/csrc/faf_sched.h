@@ -1,6 +1,7 @@
 // faf_sched.h -- host-side admission policy of the serving loop
-// (faf_serve.cpp): a first-fit device-memory arena and the scheduler that
-// turns a FIFO of pending requests into batches for free stream slots.
+// (faf_serve.cpp): a first-fit device-memory arena, the scheduler that
+// turns a FIFO of pending requests into batches for free stream slots, and
+// the router that spreads requests over several GPUs' loops.
 //
 // Pure C++17, no CUDA: the same code runs inside the library and in the CPU
 // unit test (tests/native/sched_check.cpp), which drives it with synthetic
@@ -212,6 +213,63 @@ class Scheduler {
     std::vector<int> free_slots_;
     std::set<uint64_t> busy_streams_;
     long long batches_ = 0, merged_ = 0;
+};
+
+// Request routing over several GPUs, each with its own serving loop and
+// arena (one process per GPU, or one Scheduler per device): the policy a
+// front end applies before submitting to a GPU's queue.
+//   - Requests of an ordered stream (stream_key != 0) go to the GPU that
+//     took the stream's first chunk: its overlap state lives there.
+//   - Other requests go to the GPU with the fewest bytes in flight (routed
+//     and not yet completed) among those whose arena can ever hold them;
+//     ties go to the lower index.
+//   - A request no GPU's arena can hold is rejected (-1).
+class Router {
+   public:
+    explicit Router(const std::vector<size_t>& arena_bytes) : cap_(arena_bytes) {
+        load_.assign(cap_.size(), 0);
+        routed_.assign(cap_.size(), 0);
+    }
+    int devices() const { return (int)cap_.size(); }
+    // The GPU for request r, or -1; its bytes count as in flight there.
+    int route(const SchedReq& r) {
+        const size_t need = Arena::round(r.bytes);
+        if (r.stream_key) {
+            auto it = stream_dev_.find(r.stream_key);
+            if (it != stream_dev_.end()) {
+                if (need > cap_[it->second]) return -1;
+                take(it->second, need);
+                return it->second;
+            }
+        }
+        int best = -1;
+        for (int d = 0; d < (int)cap_.size(); d++) {
+            if (need > cap_[d]) continue;
+            if (best < 0 || load_[d] < load_[best]) best = d;
+        }
+        if (best < 0) return -1;
+        if (r.stream_key) stream_dev_[r.stream_key] = best;
+        take(best, need);
+        return best;
+    }
+    // A routed request finished on GPU d.
+    void complete(int d, size_t bytes) {
+        const size_t b = Arena::round(bytes);
+        load_[d] = load_[d] > b ? load_[d] - b : 0;
+    }
+    // The stream's last chunk finished: later chunks may go anywhere.
+    void end_stream(uint64_t stream_key) { stream_dev_.erase(stream_key); }
+    size_t in_flight(int d) const { return load_[d]; }
+    long long routed(int d) const { return routed_[d]; }
+
+   private:
+    void take(int d, size_t need) {
+        load_[d] += need;
+        routed_[d]++;
+    }
+    std::vector<size_t> cap_, load_;
+    std::vector<long long> routed_;
+    std::map<uint64_t, int> stream_dev_;
 };
 
 }  // namespace fafs

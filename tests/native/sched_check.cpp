@@ -178,8 +178,52 @@ static void test_fuzz() {
     CHECK(s.arena().in_use() == 0);
 }
 
+// Router: stream affinity, least bytes in flight, capacity, completion.
+static void test_router() {
+    using fafs::Router;
+    Router rt({1 << 20, 1 << 20, 1 << 16});
+    // three equal requests spread over the three GPUs, lowest index first
+    CHECK(rt.route(R(1, 7, 4096)) == 0);
+    CHECK(rt.route(R(2, 7, 4096)) == 1);
+    CHECK(rt.route(R(3, 7, 4096)) == 2);
+    // a request larger than GPU 2's arena skips it
+    CHECK(rt.route(R(4, 7, 100000)) == 0);
+    CHECK(rt.route(R(5, 7, 4096)) == 1);
+    CHECK(rt.route(R(6, 7, 4096)) == 2);
+    // nothing can hold 2 MB
+    CHECK(rt.route(R(7, 7, 2 << 20)) == -1);
+    // a stream sticks to the GPU of its first chunk, whatever the load
+    // (GPUs 1 and 2 tie at 8192 bytes in flight: the lower index)
+    const int d = rt.route(R(8, 9, 256, 55));
+    CHECK(d == 1);
+    for (int k = 0; k < 5; k++) CHECK(rt.route(R(9 + k, 9, 256, 55)) == d);
+    // completions lower the load and steer new requests back
+    rt.complete(0, 100000);
+    rt.complete(0, 4096);
+    CHECK(rt.in_flight(0) == 0);
+    CHECK(rt.route(R(20, 7, 4096)) == 0);
+    rt.end_stream(55);
+    CHECK(rt.routed(0) + rt.routed(1) + rt.routed(2) == 13);  // one was rejected
+    // balance: many random requests keep the loads within one request
+    Router b({1ull << 30, 1ull << 30, 1ull << 30, 1ull << 30});
+    std::mt19937 g(3);
+    size_t biggest = 0;
+    for (int i = 0; i < 4000; i++) {
+        const size_t sz = 256 + g() % (1 << 20);
+        biggest = sz > biggest ? sz : biggest;
+        CHECK(b.route(R(100 + i, g() % 5, sz)) >= 0);
+    }
+    size_t lo = SIZE_MAX, hi = 0;
+    for (int k = 0; k < 4; k++) {
+        lo = b.in_flight(k) < lo ? b.in_flight(k) : lo;
+        hi = b.in_flight(k) > hi ? b.in_flight(k) : hi;
+    }
+    CHECK(hi - lo <= Arena::round(biggest));
+}
+
 int main() {
     test_arena();
+    test_router();
     test_fifo_slots();
     test_merge();
     test_budget();
