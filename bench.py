@@ -746,7 +746,7 @@ def _bytes_of(workload, count):
         algorithmic_bytes(workload, WORKLOADS["uneven"][2])
 
 
-def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
+def cpu_baseline(workload, host_in, seconds=1.0, threads=None):
     """The reference library (oracle/_ref, built from its own sources) on the
     host cores, planned once: full-batch passes of the workload, repeated
     until `seconds` elapse, on all host threads; plus the same on one thread
@@ -771,7 +771,8 @@ def cpu_baseline(workload, host_in, seconds=10.0, threads=None):
                 "cores": 1, "kind": "port",
                 "sample": f"{reps} passes x 2 signals of the workload ({el:.1f} s, the oracle's "
                           "FP64 numpy restatement: the reference has no inverse STFT)"}
-    rr.run()  # warm
+    for _ in range(5):  # warm-up passes, as the reference arm's default
+        rr.run()
     reps, t0 = 0, time.perf_counter()
     while True:
         rr.run()
@@ -999,7 +1000,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="pipeline", choices=sorted(WORKLOADS))
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    # about the reference arm's timed span (20 full-batch passes), so that the
+    # two CPU figures see the same host clocks
+    ap.add_argument("--cpu-seconds", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-r2c", action="store_true",
                     help="skip the R2C kernel-only sub-record of the pipeline line")
