@@ -405,6 +405,23 @@ def time_steps(torch, stream, steps, fn):
     return ev0.elapsed_time(ev1) / steps
 
 
+def step_latencies(torch, stream, steps, fn):
+    """p50 / p99 / max of `steps` individually timed calls fn(i) (CUDA events
+    around each call on `stream`), in ms."""
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    torch.cuda.synchronize()
+    for i, (a, b) in enumerate(evs):
+        a.record(stream)
+        fn(i)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = np.array([a.elapsed_time(b) for a, b in evs])
+    return {"p50_ms": round(float(np.percentile(ms, 50)), 4),
+            "p99_ms": round(float(np.percentile(ms, 99)), 4),
+            "max_ms": round(float(ms.max()), 4), "steps": steps}
+
+
 def r2c_subrecord(F, torch, stream, sets, host_in, steps, peak):
     """Kernel-only R2C n=4096 on the headline's seed-1 signals (batch 8192),
     rotating over the same input sets: the >= 70 % of HBM target's line."""
@@ -519,6 +536,13 @@ def run_ours(args, rank, world, local_rank):
                                      "speedup_over_plain": round(pms / tms, 3),
                                      "max_rel_l2_vs_fp64": max(errs),
                                      "sample": f"{len(errs)} transforms across the lengths"}
+        # latency of one whole uneven batch, step by step, for the three methods
+        nlat = max(args.steps, 100)
+        plain["latency_per_batch"] = {
+            "persistent_graph": step_latencies(torch, stream, nlat, lambda i: step(i)),
+            "tensor_core_graph": step_latencies(torch, stream, nlat, lambda i: step(i, pl=ttc)),
+            "plain_one_launch_per_length": step_latencies(torch, stream, nlat,
+                                                           lambda i: step(i, plain=True))}
         for p in ttc:
             p.close()
 

@@ -195,18 +195,27 @@ bool build_size(int n, FftSize& out, std::string& err, int ct_ord) {
     if (!force_generic && n >= 16 && n <= kMaxSingleCta && (n & (n - 1)) == 0) {
         // Per-stage table for the compile-time kernels, in their radix order
         // (fafct::ct_radix: the same function the kernels use); stage s
-        // (s >= 1) with span P and radix R holds W_{PR}^{r k} at [(r - 1) P + k].
+        // (s >= 1) with span P and radix R holds W_{PR}^{r k} at [(r - 1) P + k],
+        // or, for stages that fafct::ct_split_q splits, its two short tables.
         int lg = 0;
         while ((1 << lg) < n) lg++;
         const int ns = fafct::ct_stages(lg, ct_ord);
         std::vector<float2> tws;
+        auto w = [&](long long e, int len) {
+            const double a = -2.0 * M_PI * (double)e / (double)len;
+            tws.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+        };
         for (int s = 1; s < ns; s++) {
             const int R = fafct::ct_radix(lg, ct_ord, s), P = fafct::ct_span(lg, ct_ord, s);
-            for (int r = 1; r < R; r++)
-                for (int k = 0; k < P; k++) {
-                    const double a = -2.0 * M_PI * (double)r * (double)k / (double)(P * R);
-                    tws.push_back(make_float2((float)std::cos(a), (float)std::sin(a)));
+            const int Q = fafct::ct_split_q(lg, ct_ord, s);
+            for (int r = 1; r < R; r++) {
+                if (!Q) {
+                    for (int k = 0; k < P; k++) w((long long)r * k, P * R);
+                } else {  // split stage: W^{r a Q} for a < P / Q, then W^{r b} for b < Q
+                    for (int a = 0; a < P / Q; a++) w((long long)r * a * Q, P * R);
+                    for (int b = 0; b < Q; b++) w((long long)r * b, P * R);
                 }
+            }
         }
         if (tws.empty()) tws.push_back(make_float2(1.f, 0.f));
         if (!cuda_ok(upload(&out.d_tws, tws.data(), tws.size()), err, "twiddle upload"))
@@ -306,6 +315,16 @@ static bool ring_ok(const float* x, long long dist) {
     const char* env = std::getenv("FAF_CUDA_NO_STAGING");
     if (env && env[0] == '1') return false;
     return ((unsigned long long)(size_t)x % 16 == 0) && (dist % 4 == 0);
+}
+
+// Bulk copies of a C2C input into the workspace (k2_c2c_land, power-of-two
+// lengths >= 8192): plane starts 16-byte aligned at every transform.
+static bool land_ok(const float* re, const float* im, long long dist, bool inter) {
+    const char* env = std::getenv("FAF_CUDA_NO_STAGING");
+    if (env && env[0] == '1') return false;
+    if ((unsigned long long)(size_t)re % 16) return false;
+    if (inter) return (2 * dist) % 4 == 0;
+    return (unsigned long long)(size_t)im % 16 == 0 && dist % 4 == 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -914,6 +933,9 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
         a.scale = p->scale; a.sgn = sgn; a.interleaved = interleaved ? 1 : 0;
         a.window = window;
+        a.land = (p->inner.ct_log2 >= 13 && !window && land_ok(in_re, in_im, in_dist, interleaved))
+                     ? 1 : 0;
+        a.err = p->d_wait_err;
         const int slots = p->inner.n;
         if (p->tc)
             return fafk::launch_c2c_tc(p->inner.ct_log2, p->inner.d_tws, a, p->d_tcB,

@@ -46,6 +46,18 @@ __host__ __device__ constexpr int ct_span(int lg, int ord, int s) {
     for (int j = 0; j < s; j++) p *= ct_radix(lg, ord, j);
     return p;
 }
+// Per-stage twiddle table: stage s >= 1 (radix R, span P) needs W_{PR}^{r k}
+// for r < R, k < P.  Stages with P >= 1024 store it as a product of two short
+// tables, k = a Q + b: W_{PR}^{r a Q} (a < P / Q) then W_{PR}^{r b} (b < Q), per
+// r; so the whole table of a 16384-point transform is 36 KB instead of 131,
+// small enough to live in shared memory next to the workspace.
+__host__ __device__ constexpr int ct_split_q(int lg, int ord, int s) {
+    return ct_span(lg, ord, s) >= 4096 ? 64 : ct_span(lg, ord, s) >= 1024 ? 32 : 0;
+}
+__host__ __device__ constexpr int ct_tw_len(int lg, int ord, int s) {
+    const int q = ct_split_q(lg, ord, s), P = ct_span(lg, ord, s);
+    return (ct_radix(lg, ord, s) - 1) * (q ? P / q + q : P);
+}
 
 template <int N, int ORD = 0>
 struct P2 {
@@ -57,9 +69,10 @@ struct P2 {
     static constexpr int T = N / 16;                    // threads per transform
     __host__ __device__ static constexpr int radix(int s) { return ct_radix(LOG, ORD, s); }
     __host__ __device__ static constexpr int span(int s) { return ct_span(LOG, ORD, s); }
+    __host__ __device__ static constexpr int split_q(int s) { return ct_split_q(LOG, ORD, s); }
     __host__ __device__ static constexpr int tw_offset(int s) {
         int o = 0;
-        for (int j = 1; j < s; j++) o += (radix(j) - 1) * span(j);
+        for (int j = 1; j < s; j++) o += ct_tw_len(LOG, ORD, j);
         return o;
     }
     static constexpr int TW = tw_offset(NS);            // table entries
@@ -70,6 +83,25 @@ __device__ __forceinline__ int pad2(int a) { return a + (a >> 4); }
 // float2 slots needed for `slots` complex elements
 __host__ __device__ constexpr int plane2(int slots) {
     return (slots - 1) + ((slots - 1) >> 4) + 1;
+}
+
+// Twiddle W_{PR}^{r k} of stage S (1 <= r < R, k < P) from the per-stage table
+// (shared memory when TWS_SMEM): one entry, or the product of a split stage's
+// two entries.
+template <int N, int S, bool TWS_SMEM, int ORD>
+__device__ __forceinline__ float2 stage_tw(const float2* __restrict__ tws, int k, int r) {
+    using Pl = P2<N, ORD>;
+    constexpr int P = Pl::span(S), Q = Pl::split_q(S), OFF = Pl::tw_offset(S);
+    if constexpr (Q == 0) {
+        const int i = OFF + (r - 1) * P + k;
+        return TWS_SMEM ? tws[i] : __ldg(&tws[i]);
+    } else {
+        constexpr int A = P / Q;
+        const int i = OFF + (r - 1) * (A + Q);
+        const float2 a = TWS_SMEM ? tws[i + k / Q] : __ldg(&tws[i + k / Q]);
+        const float2 b = TWS_SMEM ? tws[i + A + k % Q] : __ldg(&tws[i + A + k % Q]);
+        return make_float2(a.x * b.x - a.y * b.y, fmaf(a.x, b.y, a.y * b.x));
+    }
 }
 
 // Interleaved complex workspace.  kFast marks shared-memory sources / sinks
@@ -117,14 +149,22 @@ __device__ __forceinline__ float2* fast_ptr(const T& x) {
     else return x.s.d;
 }
 
-template <int N, int S, bool TWS_SMEM, int ORD = 0, class Src, class Snk, class Sync>
+struct NoHook {
+    __device__ __forceinline__ void operator()() const {}
+};
+
+// One Stockham stage.  `rd` runs once every value the stage reads is in
+// registers, before anything is written (a kernel that reuses the source's
+// memory starts there; the default does nothing).
+template <int N, int S, bool TWS_SMEM, int ORD = 0, class Src, class Snk, class Sync,
+          class RdHook = NoHook>
 __device__ __forceinline__ void ct_stage(float (&xr)[16], float (&xi)[16], int t,
                                          const float2* __restrict__ tws, const Src& src,
-                                         const Snk& snk, const Sync& sync) {
+                                         const Snk& snk, const Sync& sync,
+                                         const RdHook& rd = RdHook()) {
     using Pl = P2<N, ORD>;
     constexpr int R = Pl::radix(S), P = Pl::span(S), NB = N / R, T = Pl::T, MB = 16 / R;
     constexpr int LP = ilog2(P);
-    constexpr int OFF = Pl::tw_offset(S);
 #pragma unroll
     for (int i = 0; i < MB; i++) {
         const int b = t + i * T;
@@ -147,15 +187,15 @@ __device__ __forceinline__ void ct_stage(float (&xr)[16], float (&xi)[16], int t
         }
         if constexpr (S > 0) {
             const int k = b & (P - 1);
-            const float2* w = tws + OFF + k;
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                const float2 wr = TWS_SMEM ? w[(r - 1) * P] : __ldg(&w[(r - 1) * P]);
+                const float2 wr = stage_tw<N, S, TWS_SMEM, ORD>(tws, k, r);
                 cmul_inplace(xr[i * R + r], xi[i * R + r], wr.x, wr.y);
             }
         }
         Dft<R>::run(&xr[i * R], &xi[i * R]);
     }
+    rd();
     if constexpr (Src::kSmem && Snk::kSmem) sync();
 #pragma unroll
     for (int i = 0; i < MB; i++) {
@@ -203,9 +243,6 @@ struct GroupSync {
     }
 };
 
-struct NoHook {
-    __device__ __forceinline__ void operator()() const {}
-};
 
 // Stages S.. of the transform.  SKIP_LAST stops before the last stage (the
 // caller runs it, fused with what follows; the stage before it has written
@@ -294,7 +331,6 @@ __device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
                                               const Pair& pair) {
     using Pl = P2<N, ORD>;
     constexpr int S = Pl::NS - 1, R = Pl::radix(S), P = Pl::span(S), NB = N / R;
-    constexpr int OFF = Pl::tw_offset(S);
     static_assert(LastPairs<N, ORD>::ok && P == NB && Pl::T == NB / 2, "radix-8 last stage");
     const int b[2] = {t, t == 0 ? NB / 2 : NB - t};
     float xr[2][R], xi[2][R];
@@ -309,10 +345,9 @@ __device__ __forceinline__ void ct_last_pairs(int t, const float2* ws,
             xi[h][r] = v.y;
         }
         if (b[h] != 0) {
-            const float2* w = tws + OFF + b[h];
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                const float2 wr = TWS_SMEM ? w[(r - 1) * P] : __ldg(&w[(r - 1) * P]);
+                const float2 wr = stage_tw<N, S, TWS_SMEM, ORD>(tws, b[h], r);
                 cmul_inplace(xr[h][r], xi[h][r], wr.x, wr.y);
             }
         }

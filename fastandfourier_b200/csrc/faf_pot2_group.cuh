@@ -20,7 +20,9 @@ __host__ __device__ constexpr int even2(int x) { return (x + 1) & ~1; }
 
 template <int N, int ORD = 0>
 struct CtCfg {
-    static constexpr bool TW_SMEM = P2<N, ORD>::TW * 8 <= 32768;
+    // up to 56 KB: every table (36 KB for 16384-point C2C, 52 KB for the real
+    // kinds' 16384-point inner FFT, with their split stages)
+    static constexpr bool TW_SMEM = P2<N, ORD>::TW * 8 <= 57344;
     static constexpr int TWN = TW_SMEM ? even2(P2<N, ORD>::TW > 0 ? P2<N, ORD>::TW : 1) : 0;
 };
 

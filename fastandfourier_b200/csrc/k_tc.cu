@@ -158,7 +158,6 @@ __device__ __forceinline__ void tc_stage(float (&xr)[16], float (&xi)[16], int t
     using Pl = P2<N>;
     static_assert(Pl::radix(S) == 16, "tensor-core stages are radix 16");
     constexpr int P = Pl::span(S), NB = N / 16, LP = fafct::ilog2(P);
-    constexpr int OFF = Pl::tw_offset(S);
     const int b = t;
     // ---- inputs and the stage's twiddles (FP32)
     if constexpr (fafct::is_fast<Src>::value && NB % 16 == 0) {
@@ -179,10 +178,9 @@ __device__ __forceinline__ void tc_stage(float (&xr)[16], float (&xi)[16], int t
     }
     if constexpr (S > 0) {
         const int k = b & (P - 1);
-        const float2* w = tws + OFF + k;
 #pragma unroll
         for (int r = 1; r < 16; r++) {
-            const float2 wr = TWS_SMEM ? w[(r - 1) * P] : __ldg(&w[(r - 1) * P]);
+            const float2 wr = fafct::stage_tw<N, S, TWS_SMEM, 0>(tws, k, r);
             fafct::cmul_inplace(xr[r], xi[r], wr.x, wr.y);
         }
     }

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import REL_L2_TOL, seeded
+from oracle import orc
 
 pytestmark = pytest.mark.gpu
 
@@ -130,3 +131,59 @@ def test_pipeline_sizes_fused_middle(cuda, n):
     y = t.pipeline(torch.from_numpy(x).cuda()).cpu().numpy()
     want = np.fft.irfft(np.fft.rfft(x.astype(np.float64), axis=-1) * m, n=n, axis=-1)
     assert rel(y, want) <= REL_L2_TOL
+
+
+def _c2c_pair(torch, F, n, batch, inverse, inter, seed):
+    rng = seeded(seed)
+    re = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    im = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    t = F.Transform.fft(n, inverse=inverse, layout=F.L_INTERLEAVED if inter else F.L_DEFAULT)
+    if inter:
+        z = np.stack([re, im], axis=-1).reshape(batch, 2 * n)
+        y = t.c2c(torch.from_numpy(z).cuda()).cpu().numpy().reshape(batch, n, 2)
+        got = y[..., 0] + 1j * y[..., 1]
+    else:
+        yr, yi = t.c2c(torch.from_numpy(re).cuda(), torch.from_numpy(im).cuda())
+        got = yr.cpu().numpy() + 1j * yi.cpu().numpy()
+    assert t.wait_status() == 0
+    return re, im, got
+
+
+@pytest.mark.parametrize("n", [8192, 16384])
+@pytest.mark.parametrize("batch", [1, 3, 149, 300])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_c2c_landed_inputs_match_direct_loads(cuda, monkeypatch, n, batch, inverse):
+    """Power-of-two C2C of 8192 and 16384 points lands each transform's planes
+    in the workspace by bulk copy; the result equals the direct loads bit for
+    bit (same arithmetic) and FP64 within the tolerance."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    re, im, got = _c2c_pair(torch, F, n, batch, inverse, False, n + batch)
+    want = orc.fp64_c2c(re, im, inverse=inverse)
+    assert rel(got, want) <= REL_L2_TOL
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    _, _, direct = _c2c_pair(torch, F, n, batch, inverse, False, n + batch)
+    assert np.array_equal(got, direct)
+
+
+def test_c2c_landed_interleaved_and_unaligned(cuda):
+    """Interleaved 16384-point inputs land as one copy per transform; plane
+    distances that are not a multiple of 4 floats take the direct loads."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n = 16384
+    re, im, got = _c2c_pair(torch, F, n, 5, False, True, 3)
+    assert rel(got, orc.fp64_c2c(re, im)) <= REL_L2_TOL
+    batch, dist = 7, n + 2
+    rng = seeded(4)
+    xr = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    xi = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    br, bi = _strided(torch, xr, dist), _strided(torch, xi, dist)
+    yr = torch.empty(batch * n, device="cuda")
+    yi = torch.empty(batch * n, device="cuda")
+    t = F.Transform.fft(n)
+    t.execute_batched(F._buf(yr, yi, n, F.L_SPLIT), F._buf(br, bi, n, F.L_SPLIT), batch,
+                      in_dist=dist, out_dist=n)
+    got = yr.cpu().numpy().reshape(batch, n) + 1j * yi.cpu().numpy().reshape(batch, n)
+    assert rel(got, orc.fp64_c2c(xr, xi)) <= REL_L2_TOL
+    assert t.wait_status() == 0
