@@ -9,6 +9,7 @@
 #include <algorithm>
 
 #include "faf_kernels_common.cuh"
+#include "faf_land.cuh"
 #include "faf_pot2.cuh"
 #include "faf_pot2_group.cuh"
 #include "faf_ring.cuh"
@@ -91,94 +92,32 @@ __global__ void __launch_bounds__(1024) k2_c2c(const float2* __restrict__ tws, c
     }
 }
 
-// A transform's input landed linearly at the start of its group's
-// workspace: split planes re[N] then im[N], or N interleaved (re, im) pairs.
-// Stage 0 reads it all before its barrier and then overwrites it (kSmem).
-struct LandSrc {
-    const float* d;
-    int n;
-    int inter;
-    float sgn;
-    static constexpr bool kSmem = true;
-    __device__ __forceinline__ cf get(int i) const {
-        if (inter) {
-            const float2 v = reinterpret_cast<const float2*>(d)[i];
-            return cf{v.x, sgn * v.y};
-        }
-        return cf{d[i], sgn * d[n + i]};
-    }
-};
-
 // C2C of power-of-two lengths whose groups fill a CTA (N >= 8192): the first
 // stage's 32 scalar global loads per thread, one transform per group and no
 // other transform to overlap them with, left the kernel waiting on memory.
-// Here each transform's input lands in its group's workspace by one or two
-// bulk copies (completing on the group's mbarrier), issued for the group's
-// next transform as soon as the last stage has read the workspace, so the
-// copy runs during the last stage and the stores.
+// Here each transform's input lands in its group's workspace by bulk copy
+// (faf_land.cuh), issued for the group's next transform as soon as the last
+// stage has read the workspace, so the copy runs during the last stage and
+// the stores.
 template <int N>
 __global__ void __launch_bounds__(1024) k2_c2c_land(const float2* __restrict__ tws,
                                                     const C2CArgs a, int G) {
     extern __shared__ float4 smem4[];
     CtGroup<N> q(reinterpret_cast<float2*>(smem4), N, tws);
-    __shared__ uint64_t bar[16];
-    __shared__ int failed;
+    __shared__ LandCtl ctl;
     constexpr int NS = P2<N>::NS;
     const int fpe = a.interleaved ? 2 : 1;
-    float* land = reinterpret_cast<float*>(q.ws);
-    const unsigned mb = fafct::smem_addr(&bar[q.g]);
-    // thread 0 of the group: transform b's input into the workspace
-    auto issue = [&](long long b) {
-        if (*(volatile int*)&failed) return false;
-        const long long io = b * a.in_dist * fpe;
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
-                     "r"((unsigned)(N * 8)) : "memory");
-        const unsigned dst = fafct::smem_addr(land);
-        if (a.interleaved) {
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
-                         "[%0], [%1], %2, [%3];" ::"r"(dst), "l"(a.in_re + io),
-                         "r"((unsigned)(N * 8)), "r"(mb) : "memory");
-        } else {
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
-                         "[%0], [%1], %2, [%3];" ::"r"(dst), "l"(a.in_re + io),
-                         "r"((unsigned)(N * 4)), "r"(mb) : "memory");
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
-                         "[%0], [%1], %2, [%3];" ::"r"(dst + N * 4u), "l"(a.in_im + io),
-                         "r"((unsigned)(N * 4)), "r"(mb) : "memory");
-        }
-        return true;
-    };
-    if (q.t == 0)
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
-    if (threadIdx.x == 0) failed = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    Lander<N> L{&ctl, q.g, reinterpret_cast<float*>(q.ws)};
+    L.init(q.t);
     __syncthreads();
     const long long stride = (long long)gridDim.x * G;
     long long b = (long long)blockIdx.x * G + q.g;
-    // copies issued and copies waited for, by this group (thread 0's view)
-    int issued = 0, waited = 0;
-    if (q.t == 0 && b < a.batch && issue(b)) issued++;
+    if (q.t == 0 && b < a.batch) L.issue(a, b);
     for (; b - q.g < a.batch; b += stride) {  // the same trip count for every group
         const bool live = b < a.batch;
-        if (live) {
-            bool ok = false;
-            for (int i = 0; i < fafct::kRingSpin && !*(volatile int*)&failed; i++)
-                if (fafct::mbar_test(&bar[q.g], (unsigned)(waited & 1))) {
-                    ok = true;
-                    break;
-                }
-            if (ok) {
-                waited++;
-            } else if (q.t == 0) {
-                *(volatile int*)&failed = 1;
-                if (a.err) atomicOr(a.err, 2);
-            }
-        }
-        const long long bi = live ? b : 0;
-        const long long oo = bi * a.out_dist * fpe;
-        fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, LandSrc{land, N, a.interleaved, a.sgn},
-                                          q.sync);
+        if (live) L.wait(a, q.t);
+        const long long oo = (live ? b : 0) * a.out_dist * fpe;
+        fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, L.src(a), q.sync);
         float xr[16], xi[16];
         const long long bn = b + stride;
         fafct::ct_stage<N, NS - 1, kTw<N>, 0>(
@@ -188,14 +127,10 @@ __global__ void __launch_bounds__(1024) k2_c2c_land(const float2* __restrict__ t
                                               a.sgn, a.interleaved, live}},
             q.sync, [&]() {
                 q.sync();  // the whole group has read the workspace
-                if (q.t == 0 && bn < a.batch && issue(bn)) issued++;
+                if (q.t == 0 && bn < a.batch) L.issue(a, bn);
             });
     }
-    // after a wait ran out, no copy may still be in flight when the CTA exits
-    if (q.t == 0 && issued > waited) {
-        for (int i = 0; i < fafct::kRingSpin; i++)
-            if (fafct::mbar_test(&bar[q.g], (unsigned)((issued - 1) & 1))) break;
-    }
+    L.drain(q.t);
 }
 
 // Post-pass over bin pairs after the forward FFT left Z in the workspace.

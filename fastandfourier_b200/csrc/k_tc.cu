@@ -30,6 +30,7 @@
 
 #include <algorithm>
 
+#include "faf_land.cuh"
 #include "faf_kernels_common.cuh"
 #include "faf_pot2.cuh"
 #include "faf_pot2_group.cuh"
@@ -260,33 +261,37 @@ __device__ __forceinline__ void tc_stage(float (&xr)[16], float (&xi)[16], int t
     if constexpr (Snk::kSmem) __syncthreads();
 }
 
-template <int N, int S, bool TWS, class Src, class Snk>
+// `rd` runs in the last stage once it has read the workspace (CUDA-core
+// stages only: a last stage of radix 16 takes no hook).
+template <int N, int S, bool TWS, class Src, class Snk, class RdHook = fafct::NoHook>
 __device__ __forceinline__ void any_stage(float (&xr)[16], float (&xi)[16], int t,
                                           const float2* __restrict__ tws, const Src& src,
-                                          const Snk& snk, Ctx& c) {
-    if constexpr (P2<N>::radix(S) == 16)
+                                          const Snk& snk, Ctx& c, const RdHook& rd = RdHook()) {
+    if constexpr (P2<N>::radix(S) == 16) {
+        static_assert(std::is_same_v<RdHook, fafct::NoHook>, "no hook in a tensor-core stage");
         tc_stage<N, S, TWS>(xr, xi, t, tws, src, snk, c);
-    else
-        fafct::ct_stage<N, S, TWS>(xr, xi, t, tws, src, snk, CtaSync{});
+    } else {
+        fafct::ct_stage<N, S, TWS>(xr, xi, t, tws, src, snk, CtaSync{}, rd);
+    }
 }
 
-template <int N, int S, bool TWS, class Src, class Snk>
+template <int N, int S, bool TWS, class Src, class Snk, class RdHook = fafct::NoHook>
 __device__ __forceinline__ void tc_run(float (&xr)[16], float (&xi)[16], int t, float2* ws,
                                        const float2* __restrict__ tws, const Src& src,
-                                       const Snk& snk, Ctx& c) {
+                                       const Snk& snk, Ctx& c, const RdHook& rd = RdHook()) {
     using Pl = P2<N>;
     const SmemC mid{ws};
     const LastC<Snk> last{snk};
     if constexpr (Pl::NS == 1) {
-        any_stage<N, 0, TWS>(xr, xi, t, tws, src, last, c);
+        any_stage<N, 0, TWS>(xr, xi, t, tws, src, last, c, rd);
     } else if constexpr (S == 0) {
         any_stage<N, 0, TWS>(xr, xi, t, tws, src, mid, c);
-        tc_run<N, 1, TWS>(xr, xi, t, ws, tws, mid, snk, c);
+        tc_run<N, 1, TWS>(xr, xi, t, ws, tws, mid, snk, c, rd);
     } else if constexpr (S == Pl::NS - 1) {
-        any_stage<N, S, TWS>(xr, xi, t, tws, mid, last, c);
+        any_stage<N, S, TWS>(xr, xi, t, tws, mid, last, c, rd);
     } else {
         any_stage<N, S, TWS>(xr, xi, t, tws, mid, mid, c);
-        tc_run<N, S + 1, TWS>(xr, xi, t, ws, tws, mid, snk, c);
+        tc_run<N, S + 1, TWS>(xr, xi, t, ws, tws, mid, snk, c, rd);
     }
 }
 
@@ -300,7 +305,10 @@ constexpr size_t smem_bytes() {
            (size_t)G * group_stride(N, N) * sizeof(float2) + kTailBytes;
 }
 
-template <int N>
+// LAND (8192 and 16384 points): inputs land in the workspace by bulk copy
+// (faf_land.cuh), the next transform's copy issued once the last stage has
+// read the workspace.
+template <int N, bool LAND>
 __global__ void __launch_bounds__(kThreads, 1)
     k2_c2c_tc(const float2* __restrict__ tws, const C2CArgs a, const uint4* __restrict__ gB,
               int* err) {
@@ -312,6 +320,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ float4 smem4[];
     float2* sm2 = reinterpret_cast<float2*>(smem4);
     CtGroup<N> q(sm2, N, tws);
+    __shared__ LandCtl lctl;
+    Lander<N> L{&lctl, q.g, reinterpret_cast<float*>(q.ws)};
+    if constexpr (LAND) L.init(q.t);
     uint8_t* wsb = reinterpret_cast<uint8_t*>(sm2 + CtCfg<N>::TWN);
     uint8_t* bsm = wsb + (size_t)G * group_stride(N, N) * sizeof(float2);
     uint64_t* bars = reinterpret_cast<uint64_t*>(bsm + kBBytes);
@@ -347,19 +358,33 @@ __global__ void __launch_bounds__(kThreads, 1)
     c.leader = (threadIdx.x & 127) == 0;
     float xr[16], xi[16];
     const int fpe = a.interleaved ? 2 : 1;
+    if constexpr (LAND) {
+        const long long b0 = (long long)blockIdx.x * G + q.g;
+        if (q.t == 0 && b0 < a.batch) L.issue(a, b0);
+    }
     CT_FOR_GROUPS(G, a.batch) {
         const long long b = grp_ * G + q.g;
         const bool live = b < a.batch;
         const long long bi = live ? b : 0;
         const long long io = (a.offs ? a.offs[bi] : bi * a.in_dist) * fpe;
         const long long oo = (a.offs ? a.offs[bi] : bi * a.out_dist) * fpe;
-        SplitSrc src{a.in_re + io, a.interleaved ? nullptr : a.in_im + io, a.window, a.sgn,
-                     a.interleaved, live};
         SplitSink snk{a.out_re + oo, a.interleaved ? nullptr : a.out_im + oo, a.scale, a.sgn,
                       a.interleaved, live};
         __syncthreads();  // the workspace is free (previous group done)
-        tc_run<N, 0, kTw<N>>(xr, xi, q.t, q.ws, q.tw, src, snk, c);
+        if constexpr (LAND) {
+            if (live) L.wait(a, q.t);
+            const long long bn = b + (long long)gridDim.x * G;
+            tc_run<N, 0, kTw<N>>(xr, xi, q.t, q.ws, q.tw, L.src(a), snk, c, [&]() {
+                __syncthreads();  // every group has read its workspace
+                if (q.t == 0 && bn < a.batch) L.issue(a, bn);
+            });
+        } else {
+            SplitSrc src{a.in_re + io, a.interleaved ? nullptr : a.in_im + io, a.window, a.sgn,
+                         a.interleaved, live};
+            tc_run<N, 0, kTw<N>>(xr, xi, q.t, q.ws, q.tw, src, snk, c);
+        }
     }
+    if constexpr (LAND) L.drain(q.t);
     // release the accumulators once every MMA has completed
     fence_before_sync();
     __syncthreads();
@@ -372,7 +397,10 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 template <int N>
 cudaError_t prepare_n() {
-    return prep(k2_c2c_tc<N>, smem_bytes<N>());
+    cudaError_t e = prep(k2_c2c_tc<N, false>, smem_bytes<N>());
+    if constexpr (N >= 8192)
+        if (e == cudaSuccess) e = prep(k2_c2c_tc<N, true>, smem_bytes<N>());
+    return e;
 }
 
 template <int N>
@@ -385,7 +413,13 @@ cudaError_t launch_n(const float2* tws, const C2CArgs& a, const void* gB, int* e
     constexpr int G = kThreads / P2<N>::T;
     const long long groups = (a.batch + G - 1) / G;
     const unsigned grid = (unsigned)std::max(1LL, std::min(groups, (long long)sms));
-    k2_c2c_tc<N><<<grid, kThreads, smem, st>>>(tws, a, (const uint4*)gB, err);
+    if constexpr (N >= 8192) {
+        if (a.land) {
+            k2_c2c_tc<N, true><<<grid, kThreads, smem, st>>>(tws, a, (const uint4*)gB, err);
+            return cudaGetLastError();
+        }
+    }
+    k2_c2c_tc<N, false><<<grid, kThreads, smem, st>>>(tws, a, (const uint4*)gB, err);
     return cudaGetLastError();
 }
 

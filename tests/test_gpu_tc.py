@@ -59,3 +59,18 @@ def test_tc_flag_ignored_where_unsupported(cuda):
     for n in (60, 128, 32768):
         t = F.Transform.fft(n, flags=F.FLAG_TENSOR_CORE)
         assert t.kind != "c2c-tc" and t.tc_status() == -1
+
+
+@pytest.mark.parametrize("n,batch", [(8192, 400), (16384, 300)])
+def test_tc_landed_inputs_over_several_rounds(cuda, n, batch):
+    """More transforms than SMs: every CTA lands a second (and third)
+    transform in its workspace while it finishes the previous one."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    re, im = heavy_tailed(n, batch, 900 + n)
+    t = F.Transform.fft(n, flags=F.FLAG_TENSOR_CORE)
+    yr, yi = t.c2c(torch.from_numpy(re).cuda(), torch.from_numpy(im).cuda())
+    got = yr.cpu().numpy() + 1j * yi.cpu().numpy()
+    want = orc.fp64_c2c(re, im)
+    assert float(np.linalg.norm(got - want) / np.linalg.norm(want)) <= REL_L2_TOL
+    assert t.wait_status() == 0 and t.tc_status() == 0
