@@ -239,10 +239,14 @@ def measured_hbm_peak():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+# committed ncu summary of each workload's dominant kernel
+PROFILES = {"uneven": "uneven_config3", "c2c16384tc": "c2c_tc_16384"}
+
+
 def ncu_traffic(workload):
     """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (profiles/<workload>.md, line `traffic_per_launch_bytes: X`)."""
-    p = os.path.join(ROOT, "profiles", f"{workload}.md")
+    summary (profiles/<name>.md, line `traffic_per_launch_bytes: X`)."""
+    p = os.path.join(ROOT, "profiles", f"{PROFILES.get(workload, workload)}.md")
     try:
         with open(p) as f:
             for line in f:
@@ -591,7 +595,9 @@ def run_ours(args, rank, world, local_rank):
                 "traffic": ncu_traffic(workload),
                 "algorithmic_bytes_per_launch": nbytes,
                 "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
-                           "uneven": "k_large_pot2 (the 65536-point class)", "c2c16384tc": "k2_c2c_tc",
+                           "uneven": "k4p_col (65536-point class, column pass; traffic of one "
+                                     "128-transform chunk)",
+                           "c2c16384": "k2_c2c_land", "c2c16384tc": "k2_c2c_tc",
                            "c2c4096fp64": "k64_c2c", "istft": "k2_c2r + k_ola",
                            "cwt": "k2_c2r (bank rows) + k2_r2c",
                            "icwt": "k2_r2c (rows) + k_icwt_acc + k2_c2r"}.get(
