@@ -2,14 +2,14 @@
 // one CTA (n = N1 * N2: 32768 = 128 x 256, 65536 = 256 x 256), spread over
 // many CTAs per transform in two passes through a scratch buffer:
 //
-//   pass 1 (k4p_col): a CTA takes W = 1024 / (N1/16) columns of one
+//   pass 1 (k4p_col): a CTA takes W = TH / (N1/16) columns of one
 //     transform: a cooperative load with the column index fastest across
 //     lanes (coalesced rows of W floats) transposes them into one shared
 //     workspace per column; each column runs an N1-point FFT on the
 //     compile-time engine; a cooperative copy-out multiplies the middle
 //     twiddle W_n^{col k1} (table laid out [k1][col]) and stores
 //     S[k1 * N2 + col], again W consecutive floats per row.
-//   pass 2 (k4p_row): a CTA takes W2 = 1024 / (N2/16) rows of S (contiguous,
+//   pass 2 (k4p_row): a CTA takes W2 = TH / (N2/16) rows of S (contiguous,
 //     read straight into the engine), runs N2-point FFTs, and a cooperative
 //     copy-out stores X[k1 + N1 k2] with the row index fastest (W2 consecutive
 //     floats per k2).
@@ -20,6 +20,7 @@
 // apart, so the transposing accesses of a warp (lanes on consecutive
 // columns) hit distinct banks.
 #include <algorithm>
+#include <cstdlib>
 
 #include "faf_kernels_common.cuh"
 #include "faf_pot2.cuh"
@@ -33,13 +34,13 @@ using fafct::ct_fft;
 using fafct::pad2;
 using fafct::SmemC;
 
-constexpr int kThreads = 1024;
 constexpr long long kScratchBytes = 64ll << 20;  // per chunk: stays in L2 between passes
 
-template <int N>
+// TH threads per CTA (1024, or 512 with two CTAs per SM)
+template <int N, int TH = 1024>
 struct Cols {
     static constexpr int T = P2<N>::T;         // threads per sub-FFT
-    static constexpr int W = kThreads / T;     // sub-FFTs per CTA
+    static constexpr int W = TH / T;           // sub-FFTs per CTA
     static constexpr int STR = plane2(N) | 1;  // float2 between workspaces (odd)
     static constexpr size_t smem() {
         return (size_t)CtCfg<N>::TWN * sizeof(float2) + (size_t)W * STR * sizeof(float2);
@@ -83,10 +84,10 @@ __device__ __forceinline__ long long xform_off(const Large2Args& a, long long b,
     return b * (out ? a.out_dist : a.in_dist);
 }
 
-template <int N1, int N2>
-__global__ void __launch_bounds__(kThreads, 1)
+template <int N1, int N2, int TH>
+__global__ void __launch_bounds__(TH, 1024 / TH)
     k4p_col(const Large2Args a, long long b0, long long nb) {
-    constexpr int W = Cols<N1>::W, STR = Cols<N1>::STR, NCB = N2 / W;
+    constexpr int W = Cols<N1, TH>::W, STR = Cols<N1>::STR, NCB = N2 / W;
     constexpr long long n = (long long)N1 * N2;
     extern __shared__ float4 smem4[];
     Setup<N1> q(reinterpret_cast<float2*>(smem4), a.tws1);
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const float* xr = a.in_re + off + c0;
         const float* xi = a.in_im + off + c0;
         __syncthreads();  // the workspaces are free
-        for (int e = threadIdx.x; e < N1 * W; e += kThreads) {
+        for (int e = threadIdx.x; e < N1 * W; e += TH) {
             const int row = e / W, col = e % W;
             q.ws0[col * STR + pad2(row)] =
                 make_float2(__ldcs(xr + (long long)row * N2 + col),
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         __syncthreads();
         float* sr = a.scratch + bl * 2 * n;
         float* si = sr + n;
-        for (int e = threadIdx.x; e < N1 * W; e += kThreads) {
+        for (int e = threadIdx.x; e < N1 * W; e += TH) {
             const int k1 = e / W, col = e % W;
             const float2 v = q.ws0[col * STR + pad2(k1)];
             const int o = k1 * N2 + c0 + col;
@@ -119,10 +120,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-template <int N1, int N2>
-__global__ void __launch_bounds__(kThreads, 1)
+template <int N1, int N2, int TH>
+__global__ void __launch_bounds__(TH, 1024 / TH)
     k4p_row(const Large2Args a, long long b0, long long nb) {
-    constexpr int W = Cols<N2>::W, STR = Cols<N2>::STR, NRB = N1 / W;
+    constexpr int W = Cols<N2, TH>::W, STR = Cols<N2>::STR, NRB = N1 / W;
     constexpr long long n = (long long)N1 * N2;
     extern __shared__ float4 smem4[];
     Setup<N2> q(reinterpret_cast<float2*>(smem4), a.tws2);
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         float* yr = a.out_re + off + r0;
         float* yi = a.out_im + off + r0;
         const float sim = a.sgn * a.scale;
-        for (int e = threadIdx.x; e < N2 * W; e += kThreads) {
+        for (int e = threadIdx.x; e < N2 * W; e += TH) {
             const int k2 = e / W, g = e % W;
             const float2 v = q.ws0[g * STR + pad2(k2)];
             __stcs(yr + (long long)N1 * k2 + g, v.x * a.scale);
@@ -149,47 +150,67 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+// Threads per CTA of both passes: 512, two CTAs per SM (FAF_CUDA_4STEP_THREADS
+// =1024: one CTA of 1024).  Measured on B200: 65536-point C2C, batch 512,
+// 1636 -> 1907 GB/s; 32768, batch 1024, 1528 -> 1775; the uneven graph
+// 1651 -> 1777.  The two CTAs of an SM drift apart, so one loads its columns
+// while the other computes.
+inline int cta_threads() {
+    const char* e = std::getenv("FAF_CUDA_4STEP_THREADS");
+    return (e && atoi(e) == 1024) ? 1024 : 512;
+}
+
 // Kernel attributes (dynamic shared memory above 48 KB), set once per
 // device (prep memoises them) and before any stream capture reaches the
 // launches.
-template <int N1, int N2>
+template <int N1, int N2, int TH>
 cudaError_t prepare_pair() {
-    cudaError_t e = prep(k4p_col<N1, N2>, Cols<N1>::smem());
-    if (e == cudaSuccess) e = prep(k4p_row<N1, N2>, Cols<N2>::smem());
+    cudaError_t e = prep(k4p_col<N1, N2, TH>, Cols<N1, TH>::smem());
+    if (e == cudaSuccess) e = prep(k4p_row<N1, N2, TH>, Cols<N2, TH>::smem());
     return e;
 }
 
 // The same, and the kernels' module loaded on the current device now rather
 // than at the first launch (lazy module loading): for callers that must not
 // allocate when they launch.
-template <int N1, int N2>
+template <int N1, int N2, int TH>
 cudaError_t load_pair() {
-    cudaError_t e = prepare_pair<N1, N2>();
+    cudaError_t e = prepare_pair<N1, N2, TH>();
     cudaFuncAttributes fa;
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k4p_col<N1, N2>);
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k4p_row<N1, N2>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k4p_col<N1, N2, TH>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k4p_row<N1, N2, TH>);
     return e;
 }
 
-template <int N1, int N2>
-cudaError_t launch_pair(const Large2Args& a, cudaStream_t st) {
-    static_assert(N1 * N2 >= 16384 && N2 % Cols<N1>::W == 0 && N1 % Cols<N2>::W == 0,
+template <int N1, int N2, int TH>
+cudaError_t launch_pair_t(const Large2Args& a, cudaStream_t st) {
+    static_assert(N1 * N2 >= 16384 && N2 % Cols<N1, TH>::W == 0 && N1 % Cols<N2, TH>::W == 0,
                   "column / row blocks must tile the transform");
-    constexpr size_t sm1 = Cols<N1>::smem(), sm2 = Cols<N2>::smem();
-    cudaError_t e = prepare_pair<N1, N2>();
+    constexpr size_t sm1 = Cols<N1, TH>::smem(), sm2 = Cols<N2, TH>::smem();
+    cudaError_t e = prepare_pair<N1, N2, TH>();
     if (e != cudaSuccess) return e;
     const int sms = fafk::sm_count();
     const long long chunk = std::max(1LL, a.scratch_transforms);
     for (long long b0 = 0; b0 < a.batch; b0 += chunk) {
         const long long nb = std::min(chunk, a.batch - b0);
-        const long long t1 = nb * (N2 / Cols<N1>::W), t2 = nb * (N1 / Cols<N2>::W);
-        k4p_col<N1, N2><<<(unsigned)std::min<long long>(t1, 8LL * sms), kThreads, sm1, st>>>(
-            a, b0, nb);
-        k4p_row<N1, N2><<<(unsigned)std::min<long long>(t2, 8LL * sms), kThreads, sm2, st>>>(
-            a, b0, nb);
+        const long long t1 = nb * (N2 / Cols<N1, TH>::W), t2 = nb * (N1 / Cols<N2, TH>::W);
+        k4p_col<N1, N2, TH><<<(unsigned)std::min<long long>(t1, 8LL * sms), TH, sm1, st>>>(a, b0, nb);
+        k4p_row<N1, N2, TH><<<(unsigned)std::min<long long>(t2, 8LL * sms), TH, sm2, st>>>(a, b0, nb);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+template <int N1, int N2>
+cudaError_t launch_pair(const Large2Args& a, cudaStream_t st) {
+    return cta_threads() == 512 ? launch_pair_t<N1, N2, 512>(a, st)
+                                : launch_pair_t<N1, N2, 1024>(a, st);
+}
+
+template <int N1, int N2>
+cudaError_t load_both() {
+    cudaError_t e = load_pair<N1, N2, 1024>();
+    return e == cudaSuccess ? load_pair<N1, N2, 512>() : e;
 }
 
 }  // namespace l2p
@@ -208,9 +229,9 @@ int large_pot2_launches(int n1, int n2, long long batch) {
 }
 
 cudaError_t large_pot2_prepare(int n1, int n2) {
-    if (n1 == 128 && n2 == 128) return l2p::load_pair<128, 128>();
-    if (n1 == 128 && n2 == 256) return l2p::load_pair<128, 256>();
-    if (n1 == 256 && n2 == 256) return l2p::load_pair<256, 256>();
+    if (n1 == 128 && n2 == 128) return l2p::load_both<128, 128>();
+    if (n1 == 128 && n2 == 256) return l2p::load_both<128, 256>();
+    if (n1 == 256 && n2 == 256) return l2p::load_both<256, 256>();
     return cudaErrorInvalidValue;
 }
 
