@@ -423,6 +423,15 @@ struct OpsMul1 {
     const PipeOp* op;
     __device__ __forceinline__ cf operator()(int k, cf v) const { return mul_bin(*op, k, v); }
 };
+// The single MUL on bins 1 .. m - 2 of a spectrum bound over all m bins:
+// mul_bin's complex product without its guards.
+struct OpsMul1Full {
+    const PipeOp* op;
+    __device__ __forceinline__ cf operator()(int k, cf v) const {
+        const float hr = __ldg(op->hr + k), hi = __ldg(op->hi_ + k);
+        return cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
+    }
+};
 __host__ __device__ inline bool ops_single_mul(const RealArgs& a) {
     return a.nops == 1 && a.ops[0].code == OP_MUL;
 }

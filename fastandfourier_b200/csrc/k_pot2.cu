@@ -497,9 +497,11 @@ __device__ __forceinline__ void pipe_middle(int t, const SmemC& mid,
 // The same bin-pair pass fused with the forward transform's last stage
 // (fafct::ct_last_pairs): each thread transforms the bins it owns in
 // registers and writes the pre-pass result back to those same slots.
-template <int N, int SEL = -1, class Ops>
+// pair_ops serves the bins of the pairs (1 .. N - 1), ops DC and Nyquist.
+template <int N, int SEL = -1, class Ops, class PairOps = Ops>
 __device__ __forceinline__ void pipe_middle_fused(int t, float2* ws, const float2* tw,
-                                                  const float2* __restrict__ stw, const Ops& ops) {
+                                                  const float2* __restrict__ stw, const Ops& ops,
+                                                  const PairOps& pair_ops) {
     const SmemC mid{ws};
     fafct::ct_last_pairs<N, kTw<N, kRO>, kRO, SEL>(
         t, ws, tw,
@@ -513,8 +515,8 @@ __device__ __forceinline__ void pipe_middle_fused(int t, float2* ws, const float
             cf Xk, Xnk;
             r2c_pair(zk, zn, w, Xk, Xnk);
             if (k == N - k) Xk = Xnk;
-            Xk = ops(k, Xk);
-            Xnk = (k == N - k) ? Xk : ops(N - k, Xnk);
+            Xk = pair_ops(k, Xk);
+            Xnk = (k == N - k) ? Xk : pair_ops(N - k, Xnk);
             cf Zk, Znk;
             c2r_pair(Xk, Xnk, w, Zk, Znk);
             if (k != N - k) mid.put(k, Zk);
@@ -560,10 +562,20 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
                 fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(
                     q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, q.sync);
             }
-            if (ops_single_mul(a))
-                pipe_middle_fused<N, kR2cSel<N, RING>>(q.t, q.ws, q.tw, a.stw, OpsMul1{&a.ops[0]});
-            else
-                pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsAny{&a});
+            if (ops_single_mul(a)) {
+                // a bound spectrum covering every bin: no guard on the pairs'
+                // bins (mul_bin's guards only act on DC and Nyquist there)
+                if (a.ops[0].m == N + 1)
+                    pipe_middle_fused<N, kR2cSel<N, RING>>(q.t, q.ws, q.tw, a.stw,
+                                                           OpsMul1{&a.ops[0]},
+                                                           OpsMul1Full{&a.ops[0]});
+                else
+                    pipe_middle_fused<N, kR2cSel<N, RING>>(q.t, q.ws, q.tw, a.stw,
+                                                           OpsMul1{&a.ops[0]},
+                                                           OpsMul1{&a.ops[0]});
+            } else {
+                pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsAny{&a}, OpsAny{&a});
+            }
         } else {
             if constexpr (RING) {
                 const RingHook hook =
