@@ -157,7 +157,9 @@ __device__ __forceinline__ void ct_r2c_post(int t, const SmemC& mid,
 // single-MUL middle: by selects (no branch splitting its warp) for the ring
 // kernels of inner length 2048, measured on B200: the n = 4096 R2C went from
 // 4641 to 5007 GB/s (no spills), the pipeline from 2369 to 2432 GB/s (despite
-// 40 bytes of spills).  Elsewhere the default (selects only for one-warp
+// 40 bytes of spills); with the unguarded multiply of a full-length spectrum,
+// 2691 against 2638 GB/s for a branch of its own (136 against 44 bytes of
+// spills).  Elsewhere the default (selects only for one-warp
 // transforms): the selects spill more at other lengths and in the direct-load
 // kernels.
 template <int N, bool RING>
@@ -562,20 +564,14 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
                 fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(
                     q.t, q.ws, q.tw, RealPairSrc{a.in_a + bi * a.in_dist, live, vec}, q.sync);
             }
-            if (ops_single_mul(a)) {
-                // a bound spectrum covering every bin: no guard on the pairs'
-                // bins (mul_bin's guards only act on DC and Nyquist there)
-                if (a.ops[0].m == N + 1)
-                    pipe_middle_fused<N, kR2cSel<N, RING>>(q.t, q.ws, q.tw, a.stw,
-                                                           OpsMul1{&a.ops[0]},
-                                                           OpsMul1Full{&a.ops[0]});
-                else
-                    pipe_middle_fused<N, kR2cSel<N, RING>>(q.t, q.ws, q.tw, a.stw,
-                                                           OpsMul1{&a.ops[0]},
-                                                           OpsMul1{&a.ops[0]});
-            } else {
+            // a single MUL by a spectrum bound over every bin: no guard on the
+            // pairs' bins (mul_bin's guards only act on DC and Nyquist there);
+            // any other program (a shorter spectrum included) runs the op loop
+            if (ops_single_mul(a) && a.ops[0].m == N + 1)
+                pipe_middle_fused<N, kR2cSel<N, RING>>(q.t, q.ws, q.tw, a.stw, OpsMul1{&a.ops[0]},
+                                                       OpsMul1Full{&a.ops[0]});
+            else
                 pipe_middle_fused<N>(q.t, q.ws, q.tw, a.stw, OpsAny{&a}, OpsAny{&a});
-            }
         } else {
             if constexpr (RING) {
                 const RingHook hook =
