@@ -69,8 +69,9 @@ WORKLOADS = {
                 16 * 1024, 5 * 1024 * 10),
     "c2c16384": ("C2C n=16384 batch 2048 forward (split planes), seed 3", 16384, 2048,
                  16 * 16384, 5 * 16384 * 14),
-    "c2c16384tc": ("C2C n=16384 batch 2048 forward, tensor-core form (radix-16 stages as FP16 "
-                   "hi+lo tcgen05 MMAs, FP32 accumulation), seed 3, 1% of entries x1e3",
+    "c2c16384tc": ("C2C n=16384 batch 2048 forward, tensor-core form (64-point DFTs as FP16 "
+                   "hi+lo tcgen05 MMAs in two passes, radix-4 on CUDA cores, FP32 accumulation), "
+                   "seed 3, 1% of entries x1e3",
                    16384, 2048, 16 * 16384, 5 * 16384 * 14),
     "stft": ("STFT Hann 1024 hop 256, 64 signals x 2^18 samples, seed 4", 1024, 64,
              None, None),
@@ -562,9 +563,24 @@ def run_ours(args, rank, world, local_rank):
         pms = time_steps(torch, stream, args.steps, lambda i: step(i, pl=[tp]))
         plain = {"value": round(nbytes / (pms * 1e-3) / 1e9, 1), "ms_per_step": round(pms, 4),
                  "speedup_of_tensor_core_form": round(pms / ms_per_step, 3)}
-        # three radix-16 stages x (16384 / 16) / 128 tiles x six 128x32x16 MMAs
-        tflops = batch * 3 * (16384 // 16 // 128) * 6 * 2 * 128 * 32 * 16 / (ms_per_step * 1e-3) / 1e12
+        # the radix-16 tensor-core kernels on the same data
+        os.environ["FAF_CUDA_TC_RADIX"] = "16"
+        try:
+            t16 = F.Transform.fft(n, flags=F.FLAG_TENSOR_CORE)
+        finally:
+            del os.environ["FAF_CUDA_TC_RADIX"]
+        t16.set_stream(stream)
+        for i in range(3):
+            step(i, pl=[t16])
+        ms16 = time_steps(torch, stream, args.steps, lambda i: step(i, pl=[t16]))
+        plain["radix16_tensor_core_form"] = {
+            "value": round(nbytes / (ms16 * 1e-3) / 1e9, 1), "ms_per_step": round(ms16, 4),
+            "kernel": "k2_c2c_tc", "tc_status": t16.tc_status()}
+        t16.close()
+        # two stages x two M=128 tiles x 8 K steps x 3 products of 128x128x16
+        tflops = batch * 2 * 2 * 8 * 3 * 2 * 128 * 128 * 16 / (ms_per_step * 1e-3) / 1e12
         acc["tensor_tflops"] = round(tflops, 1)
+        acc["plan_kind"] = t.kind
         tp.close()
 
     peak, peak_kind = measured_hbm_peak()
@@ -597,7 +613,7 @@ def run_ours(args, rank, world, local_rank):
                 "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
                            "uneven": "k4p_col (65536-point class, column pass; traffic of one "
                                      "128-transform chunk)",
-                           "c2c16384": "k2_c2c_land", "c2c16384tc": "k2_c2c_tc",
+                           "c2c16384": "k2_c2c_land", "c2c16384tc": "k2_c2c_tc64",
                            "c2c4096fp64": "k64_c2c", "istft": "k2_c2r + k_ola",
                            "cwt": "k2_c2r (bank rows) + k2_r2c",
                            "icwt": "k2_r2c (rows) + k_icwt_acc + k2_c2r"}.get(

@@ -699,7 +699,7 @@ extern "C" const char* faf_cuda_plan_kind(const faf_transform* t) {
     DevicePlan* p = plan_of(t);
     if (!p) return nullptr;
     switch (p->kind) {
-    case Kind::C2C: return p->tc ? "c2c-tc" : "c2c";
+    case Kind::C2C: return p->tc ? (p->d_tc64 ? "c2c-tc64" : "c2c-tc") : "c2c";
     case Kind::C2C_LARGE: return "c2c-4step";
     case Kind::RADER: return "rader";
     case Kind::BLUESTEIN: return "bluestein";

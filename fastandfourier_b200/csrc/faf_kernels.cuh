@@ -253,5 +253,12 @@ bool tc_supported(int log2n);
 cudaError_t prepare_c2c_tc(int log2n);  // kernel attributes, before any capture
 cudaError_t launch_c2c_tc(int log2n, const float2* tws, const C2CArgs& a, const void* gB,
                           int* err, cudaStream_t st);
+// Its radix-64 kernels for 4096, 8192 and 16384 points (k_tc64.cu); `tab` is
+// the plan's table of tc64_table_bytes() bytes.
+bool tc64_supported(int log2n);
+size_t tc64_table_bytes();
+cudaError_t prepare_c2c_tc64(int log2n);
+cudaError_t launch_c2c_tc64(int log2n, const C2CArgs& a, const void* tab, int* err,
+                            cudaStream_t st);
 
 }  // namespace fafk

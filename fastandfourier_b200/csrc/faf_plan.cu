@@ -363,6 +363,7 @@ void plan_free(DevicePlan* p) {
     cudaFree(p->d_tw64);
     cudaFree(p->d_stw64);
     cudaFree(p->d_tcB);
+    cudaFree(p->d_tc64);
     cudaFree(p->d_tc_err);
     cudaFree(p->d_wait_err);
     cudaFree(p->d_stage);
@@ -493,6 +494,67 @@ static bool build_tc_tables(DevicePlan* p, std::string& err) {
     return true;
 }
 
+// Tables of the radix-64 form (k_tc64.cu): one buffer laid out as the
+// kernel's shared memory from its B offset.
+//   B hi, B lo: the 64-point forward DFT as a 128 x 128 real matrix for
+//     D = A B^T with A rows (re z_0, im z_0, re z_1, ...) and D rows
+//     (re Y_0, im Y_0, ...): B[2m][2j] = cos t, B[2m][2j+1] = sin t,
+//     B[2m+1][2j] = -sin t, B[2m+1][2j+1] = cos t, t = 2 pi (j m mod 64) / 64
+//     (FP64), split into FP16 hi = fp16(B) and lo = fp16(B - hi), K-major
+//     without swizzle: element (n, k) at byte
+//     (n % 8) * 16 + (n / 8) * 128 + (k / 8) * 2048 + (k % 8) * 2;
+//   W_{64 R0}^e at [e] (256 entries), W_N^{16 b a} at [b * 4 R0 + a] and
+//     W_N^{b c} at [b * 16 + c] (1024 entries each), FP32 from FP64,
+// where N = 4096 R0.
+static bool build_tc64_tables(DevicePlan* p, int log2n, std::string& err) {
+    const int n = 1 << log2n, r0 = n / 4096;
+    std::vector<uint8_t> buf(fafk::tc64_table_bytes(), 0);
+    uint16_t* h = reinterpret_cast<uint16_t*>(buf.data());
+    const size_t half_tile = 128 * 128;
+    for (int row = 0; row < 128; row++)
+        for (int k = 0; k < 128; k++) {
+            const int m = row >> 1, j = k >> 1;
+            const double t = 2.0 * M_PI * (double)((j * m) % 64) / 64.0;
+            const double c = std::cos(t), s = std::sin(t);
+            const double v = (row & 1) == 0 ? ((k & 1) == 0 ? c : s) : ((k & 1) == 0 ? -s : c);
+            const __half hi = __double2half(v);
+            const __half lo = __double2half(v - (double)__half2float(hi));
+            const size_t idx = ((size_t)(row % 8) * 16 + (size_t)(row / 8) * 128 +
+                                (size_t)(k / 8) * 2048 + (size_t)(k % 8) * 2) / 2;
+            h[idx] = __half_as_ushort(hi);
+            h[half_tile + idx] = __half_as_ushort(lo);
+        }
+    float2* w = reinterpret_cast<float2*>(buf.data() + 4 * half_tile);
+    auto root = [](long long e, long long m) {
+        const double a = -2.0 * M_PI * (double)(e % m) / (double)m;
+        return make_float2((float)std::cos(a), (float)std::sin(a));
+    };
+    for (int e = 0; e < 256; e++) w[e] = root(e, 64LL * r0);
+    for (int b = 0; b < 64; b++) {
+        for (int a = 0; a < 4 * r0; a++) w[256 + b * 4 * r0 + a] = root(16LL * b * a, n);
+        for (int c = 0; c < 16; c++) w[256 + 1024 + b * 16 + c] = root((long long)b * c, n);
+    }
+    return cuda_ok(cudaMalloc(&p->d_tc64, buf.size()), err, "tensor-core tables") &&
+           cuda_ok(cudaMemcpy(p->d_tc64, buf.data(), buf.size(), cudaMemcpyHostToDevice), err,
+                   "tensor-core tables");
+}
+
+// The radix-64 form unless FAF_CUDA_TC_RADIX=16 asks for the radix-16 one.
+static bool want_tc64(int log2n) {
+    const char* env = std::getenv("FAF_CUDA_TC_RADIX");
+    return fafk::tc64_supported(log2n) && !(env && std::strcmp(env, "16") == 0);
+}
+
+cudaError_t tc_prepare(const DevicePlan* p) {
+    return p->d_tc64 ? fafk::prepare_c2c_tc64(p->inner.ct_log2)
+                     : fafk::prepare_c2c_tc(p->inner.ct_log2);
+}
+
+cudaError_t tc_launch(const DevicePlan* p, const fafk::C2CArgs& a, cudaStream_t st) {
+    if (p->d_tc64) return fafk::launch_c2c_tc64(p->inner.ct_log2, a, p->d_tc64, p->d_tc_err, st);
+    return fafk::launch_c2c_tc(p->inner.ct_log2, p->inner.d_tws, a, p->d_tcB, p->d_tc_err, st);
+}
+
 // FAF_CUDA_FOURSTEP_16K=1: C2C of 16384 points (without the tensor-core
 // form) on the multi-CTA two-pass four-step (128 x 128) instead of one CTA.
 static bool fourstep_16k(int n, uint32_t flags) {
@@ -532,7 +594,9 @@ DevicePlan* plan_c2c(int n, bool inverse, float scale, uint32_t flags, std::stri
         p = new_plan(Kind::C2C, n);
         if (!build_size(n, p->inner, err)) { plan_free(p); return nullptr; }
         if ((flags & FAF_FLAG_TENSOR_CORE) && p->inner.ct_log2 &&
-            fafk::tc_supported(p->inner.ct_log2) && !build_tc_tables(p, err)) {
+            fafk::tc_supported(p->inner.ct_log2) &&
+            (!build_tc_tables(p, err) ||
+             (want_tc64(p->inner.ct_log2) && !build_tc64_tables(p, p->inner.ct_log2, err)))) {
             plan_free(p);
             return nullptr;
         }
@@ -933,13 +997,14 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
         a.scale = p->scale; a.sgn = sgn; a.interleaved = interleaved ? 1 : 0;
         a.window = window;
-        a.land = (p->inner.ct_log2 >= 13 && !window && land_ok(in_re, in_im, in_dist, interleaved))
-                     ? 1 : 0;
+        // landing: the plain kernels from 8192 points, the radix-64
+        // tensor-core kernels from 4096
+        const int land_min = p->d_tc64 ? 12 : 13;
+        a.land = (p->inner.ct_log2 >= land_min && !window &&
+                  land_ok(in_re, in_im, in_dist, interleaved)) ? 1 : 0;
         a.err = p->d_wait_err;
         const int slots = p->inner.n;
-        if (p->tc)
-            return fafk::launch_c2c_tc(p->inner.ct_log2, p->inner.d_tws, a, p->d_tcB,
-                                       p->d_tc_err, st);
+        if (p->tc) return tc_launch(p, a, st);
         if (p->inner.ct_log2)
             return fafk::launch_pot2(0, p->inner.ct_log2, p->inner.d_tws, &a,
                                      geometry_ct(p->inner, slots, batch), st);

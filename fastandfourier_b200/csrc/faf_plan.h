@@ -100,6 +100,9 @@ struct DevicePlan {
     // real FP16 matrix, hi then lo, in the MMA's shared-memory layout
     bool tc = false;
     void* d_tcB = nullptr;
+    // radix-64 form (4096..16384 points, k_tc64.cu): its B operand and
+    // twiddle tables in the kernel's shared-memory layout; null = radix 16
+    void* d_tc64 = nullptr;
     int* d_tc_err = nullptr;     // set by a kernel whose MMA wait ran out
     int* d_wait_err = nullptr;   // set by a kernel whose input-ring wait ran out
     int win = 0, hop = 0;
@@ -146,6 +149,10 @@ cudaError_t exec_c2r64(DevicePlan* p, const double* Xr, const double* Xi, double
 void plan_free(DevicePlan* p);
 // Kernel launches of one exec_c2c of `batch` transforms of plan p.
 int c2c_launches(const DevicePlan* p, long long batch);
+// The tensor-core form of a C2C plan (p->tc): kernel attributes (before any
+// capture), and one batched launch (radix 64 where p->d_tc64, else radix 16).
+cudaError_t tc_prepare(const DevicePlan* p);
+cudaError_t tc_launch(const DevicePlan* p, const fafk::C2CArgs& a, cudaStream_t st);
 
 // Device-pointer executes (enqueue on `st`).
 cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, float* out_re,

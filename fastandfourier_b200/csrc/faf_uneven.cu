@@ -330,7 +330,7 @@ int build_schedule(faf_uneven* u) {
             for (int id : ids) offs.push_back(u->offsets_h[id]);
             cudaError_t e2 = upload_vec(&P.d_offs, offs);
             if (e2 == cudaSuccess)
-                e2 = p->tc ? fafk::prepare_c2c_tc(P.log2n) : fafk::prepare_pot2_c2c(P.log2n, P.g);
+                e2 = p->tc ? fafp::tc_prepare(p) : fafk::prepare_pot2_c2c(P.log2n, P.g);
             if (e2 != cudaSuccess) {
                 cudaFree(P.d_offs);
                 return cuda_fail(e2, "uneven power-of-two class");
@@ -488,8 +488,7 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
         a.scale = P.scale;
         a.sgn = u->inverse ? -1.0f : 1.0f;
         a.offs = P.d_offs;
-        e = P.plan->tc ? fafk::launch_c2c_tc(P.log2n, P.tws, a, P.plan->d_tcB,
-                                             P.plan->d_tc_err, ss)
+        e = P.plan->tc ? fafp::tc_launch(P.plan, a, ss)
                        : fafk::launch_pot2(0, P.log2n, P.tws, &a, P.g, ss);
         if (e != cudaSuccess) return e;
     }
@@ -627,6 +626,14 @@ extern "C" faf_uneven* faf_uneven_create(const size_t* lengths, size_t count,
             fail("faf_uneven_create: plan for length %d: %s", n, err.c_str());
             faf_uneven_destroy(u);
             return nullptr;
+        }
+        // The graph runs this class beside the other classes' branch.  The
+        // radix-64 tensor-core kernel takes all of an SM's shared memory
+        // (227 KB), so it would wait for SMs the other branch holds; the
+        // class takes the radix-16 kernel (143 KB) instead.
+        if (p->d_tc64) {
+            cudaFree(p->d_tc64);
+            p->d_tc64 = nullptr;
         }
         u->plans[n] = p;
         // (with 1024-thread CTAs every single-CTA length up to 16384 is one group)

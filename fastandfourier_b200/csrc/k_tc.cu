@@ -34,6 +34,7 @@
 #include "faf_kernels_common.cuh"
 #include "faf_pot2.cuh"
 #include "faf_pot2_group.cuh"
+#include "faf_tc.cuh"
 
 namespace fafk {
 namespace tc {
@@ -50,88 +51,20 @@ constexpr uint32_t kBLbo = 4 * 128;            // B: K-direction core-matrix str
 constexpr uint32_t kSbo = 128;                 // both: next 8-row group
 constexpr uint32_t kBBytes = 2 * 32 * 32 * 2;  // B hi + lo
 constexpr uint32_t kTmemCols = 32 * kWarpgroups;
-// instruction descriptor (kind::f16): D F32 (bits 4-5 = 1), A and B F16
-// (bits 7-12 = 0), both K-major (bits 15-16 = 0), N >> 3 at bit 17, M >> 4 at 24
-constexpr uint32_t kIdesc = (1u << 4) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
-constexpr int kSpinLimit = 1 << 20;
+constexpr uint32_t kIdesc = tcu::idesc_f16(128, 32);
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// Shared-memory matrix descriptor: start address, leading / stride byte
-// offsets (16-byte units), version 1 (bit 46), no swizzle.
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
-}
-
-__device__ __forceinline__ void fence_before_sync() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_after_sync() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_async_smem() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
+using tcu::commit;
+using tcu::fence_after_sync;
+using tcu::fence_async_smem;
+using tcu::fence_before_sync;
+using tcu::sdesc;
+using tcu::smem_u32;
+using tcu::split2;
+using tcu::tmem_ld32;
+using tcu::wait_bounded;
 
 __device__ __forceinline__ void mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-        "l"(a), "l"(b), "r"(kIdesc), "r"(acc)
-        : "memory");
-}
-
-__device__ __forceinline__ void commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ bool try_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Bounded wait; false when the limit ran out.
-__device__ __forceinline__ bool wait_bounded(uint64_t* bar, uint32_t parity) {
-    for (int i = 0; i < kSpinLimit; i++)
-        if (try_wait(bar, parity)) return true;
-    return false;
-}
-
-// 32 consecutive accumulator columns of this thread's TMEM lane.
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]),
-          "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]),
-          "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]),
-          "=r"(v[31])
-        : "r"(taddr)
-        : "memory");
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-// hi / lo FP16 pair of v (v already scaled into FP16 range)
-__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
-    const __half2 h = __floats2half2_rn(a, b);
-    const float2 hf = __half22float2(h);
-    const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
-    hi = *reinterpret_cast<const uint32_t*>(&h);
-    lo = *reinterpret_cast<const uint32_t*>(&l);
+    tcu::mma(d, a, b, kIdesc, acc);
 }
 
 struct Ctx {
@@ -191,10 +124,8 @@ __device__ __forceinline__ void tc_stage(float (&xr)[16], float (&xi)[16], int t
     float m = 0.f;
 #pragma unroll
     for (int r = 0; r < 16; r++) m = fmaxf(m, fmaxf(fabsf(xr[r]), fabsf(xi[r])));
-    const int e = ((__float_as_int(m) >> 23) & 0xff) - 127;
-    const int sh = max(-64, min(64, 13 - e));
-    const float s = __int_as_float((127 + sh) << 23);
-    const float inv = __int_as_float((127 - sh) << 23);
+    float s, inv;
+    tcu::pow2_scale(m, s, inv);
     {
         const uint32_t row_off = (uint32_t)((c.row & 7) * 16 + (c.row >> 3) * kSbo);
 #pragma unroll
