@@ -64,7 +64,7 @@ struct C2CArgs {
     int interleaved;
     const float* window;  // optional per-sample real window (STFT frame), or NULL
     const long long* offs = nullptr;  // per-transform element offsets (in and out), or NULL
-    // power-of-two lengths >= 8192: each transform's input lands in its
+    // power-of-two lengths >= 1024: each transform's input lands in its
     // group's workspace by bulk copy (inputs 16-byte aligned, distance a
     // multiple of 4 floats, no window, no offsets); err records a wait that
     // ran out

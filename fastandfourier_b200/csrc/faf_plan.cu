@@ -318,7 +318,7 @@ static bool ring_ok(const float* x, long long dist) {
 }
 
 // Bulk copies of a C2C input into the workspace (k2_c2c_land, power-of-two
-// lengths >= 8192): plane starts 16-byte aligned at every transform.
+// lengths >= 1024): plane starts 16-byte aligned at every transform.
 static bool land_ok(const float* re, const float* im, long long dist, bool inter) {
     const char* env = std::getenv("FAF_CUDA_NO_STAGING");
     if (env && env[0] == '1') return false;
@@ -997,9 +997,9 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
         a.scale = p->scale; a.sgn = sgn; a.interleaved = interleaved ? 1 : 0;
         a.window = window;
-        // landing: the plain kernels from 8192 points, the radix-64
-        // tensor-core kernels from 4096
-        const int land_min = p->d_tc64 ? 12 : 13;
+        // landing from 1024 points (the tensor-core kernels: radix 64 from
+        // 4096, radix 16 from 8192)
+        const int land_min = p->tc ? (p->d_tc64 ? 12 : 13) : 10;
         a.land = (p->inner.ct_log2 >= land_min && !window &&
                   land_ok(in_re, in_im, in_dist, interleaved)) ? 1 : 0;
         a.err = p->d_wait_err;

@@ -92,9 +92,9 @@ __global__ void __launch_bounds__(1024) k2_c2c(const float2* __restrict__ tws, c
     }
 }
 
-// C2C of power-of-two lengths whose groups fill a CTA (N >= 8192): the first
-// stage's 32 scalar global loads per thread, one transform per group and no
-// other transform to overlap them with, left the kernel waiting on memory.
+// C2C of power-of-two lengths from 1024 points (at most 16 groups, one
+// mbarrier each): the first stage's scalar global loads, with few transforms
+// per CTA to overlap them with, left the kernel waiting on memory.
 // Here each transform's input lands in its group's workspace by bulk copy
 // (faf_land.cuh), issued for the group's next transform as soon as the last
 // stage has read the workspace, so the copy runs during the last stage and
@@ -626,7 +626,7 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     switch (kind) {
     case 0: {
         const C2CArgs& a = *(const C2CArgs*)args;
-        if constexpr (N >= 8192) {
+        if constexpr (N >= 1024) {
             if (a.land) {
                 if ((e = prep(k2_c2c_land<N>, g.smem)) != cudaSuccess) return e;
                 k2_c2c_land<N><<<persistent_grid(k2_c2c_land<N>, g, a.batch), g.threads, g.smem,

@@ -149,11 +149,11 @@ def _c2c_pair(torch, F, n, batch, inverse, inter, seed):
     return re, im, got
 
 
-@pytest.mark.parametrize("n", [8192, 16384])
-@pytest.mark.parametrize("batch", [1, 3, 149, 300])
+@pytest.mark.parametrize("n", [1024, 2048, 4096, 8192, 16384])
+@pytest.mark.parametrize("batch", [1, 3, 149, 300, 1500])
 @pytest.mark.parametrize("inverse", [False, True])
 def test_c2c_landed_inputs_match_direct_loads(cuda, monkeypatch, n, batch, inverse):
-    """Power-of-two C2C of 8192 and 16384 points lands each transform's planes
+    """Power-of-two C2C of 1024 to 16384 points lands each transform's planes
     in the workspace by bulk copy; the result equals the direct loads bit for
     bit (same arithmetic) and FP64 within the tolerance."""
     import fastandfourier_b200 as F
