@@ -1,14 +1,19 @@
 // faf_land.cuh -- a C2C transform's input landed in its group's workspace by
-// bulk copies (k2_c2c_land, k2_c2c_tc for 8192 / 16384 points).
+// bulk copies (k2_c2c_land, the tensor-core kernels).
 //
 // One transform per group fills the workspace, so there is no room for a
 // separate input ring.  Instead each transform's planes are copied to the
-// start of the workspace (re[N] then im[N], or N interleaved pairs), the
-// first stage reads them there and overwrites them after its barrier, and
-// the copy of the group's next transform is issued as soon as the last stage
-// has read the workspace.  The copy completes on the group's mbarrier; every
-// wait is bounded, and after one runs out the kernel records the failure,
-// issues nothing more and drains what it issued before it exits.
+// start of the workspace (re, then im kPl floats further on, or the
+// interleaved pairs), the first stage reads them there and overwrites them
+// after its barrier, and the copy of the group's next transform is issued as
+// soon as the last stage has read the workspace.  A bulk copy moves whole
+// 16-byte blocks, so a plane whose start is not 16-byte aligned is copied
+// from the block boundary at or below its start, and read `head` floats in;
+// the blocks read beyond the plane share its 16-byte blocks, so they never
+// reach another page.  Every distance, offset list and base alignment lands
+// this way.  The copy completes on the group's mbarrier; every wait is
+// bounded, and after one runs out the kernel records the failure, issues
+// nothing more and drains what it issued before it exits.
 #pragma once
 
 #include "faf_kernels_common.cuh"
@@ -19,17 +24,17 @@ namespace fafk {
 // The landed input as the first stage's source (shared memory: the stage
 // reads it all before its barrier, then writes over it).
 struct LandSrc {
-    const float* d;
-    int n;
+    const float* re;  // first element of the real plane (or of the pairs)
+    const float* im;  // first element of the imaginary plane
     int inter;
     float sgn;
     static constexpr bool kSmem = true;
     __device__ __forceinline__ cf get(int i) const {
         if (inter) {
-            const float2 v = reinterpret_cast<const float2*>(d)[i];
+            const float2 v = reinterpret_cast<const float2*>(re)[i];
             return cf{v.x, sgn * v.y};
         }
-        return cf{d[i], sgn * d[n + i]};
+        return cf{re[i], sgn * im[i]};
     }
 };
 
@@ -39,9 +44,11 @@ struct LandCtl {  // static shared memory of a landing kernel
 };
 
 // One group's landing: its mbarrier and workspace.  `issued` is counted by
-// the group's thread 0, `waited` by every thread of the group.
+// the group's thread 0, `waited` by every thread of the group.  The
+// workspace holds 2 N + 8 floats.
 template <int N>
 struct Lander {
+    static constexpr int kPl = N + 4;  // floats from the landed real plane to the imaginary one
     LandCtl* ctl;
     int g;
     float* land;
@@ -56,31 +63,42 @@ struct Lander {
         if (threadIdx.x == 0) ctl->failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // Transform b's planes in global memory.
+    __device__ __forceinline__ static const float* plane(const C2CArgs& a, long long b, int p) {
+        const long long io = (a.offs ? a.offs[b] : b * a.in_dist) * (a.interleaved ? 2 : 1);
+        return (p == 0 ? a.in_re : a.in_im) + io;
+    }
+    __device__ __forceinline__ static unsigned head_bytes(const float* p) {
+        return (unsigned)(reinterpret_cast<uintptr_t>(p) & 15u);
+    }
+    __device__ __forceinline__ static void copy(unsigned dst, const float* src, unsigned bytes,
+                                                unsigned mb) {
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                     "[%0], [%1], %2, [%3];" ::"r"(dst),
+                     "l"(src), "r"(bytes), "r"(mb)
+                     : "memory");
+    }
     // Thread 0 of the group: transform b's input into the workspace.
     __device__ __forceinline__ void issue(const C2CArgs& a, long long b) {
         if (*(volatile int*)&ctl->failed) return;
         const unsigned mb = fafct::smem_addr(&ctl->bar[g]);
-        const long long io = b * a.in_dist * (a.interleaved ? 2 : 1);
         const unsigned dst = fafct::smem_addr(land);
+        const float* p0 = plane(a, b, 0);
+        const unsigned h0 = head_bytes(p0);
+        const unsigned n0 = (h0 + (a.interleaved ? 8u : 4u) * N + 15u) & ~15u;
+        unsigned n1 = 0, h1 = 0;
+        const float* p1 = nullptr;
+        if (!a.interleaved) {
+            p1 = plane(a, b, 1);
+            h1 = head_bytes(p1);
+            n1 = (h1 + 4u * N + 15u) & ~15u;
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
-                     "r"((unsigned)(N * 8))
+                     "r"(n0 + n1)
                      : "memory");
-        if (a.interleaved) {
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
-                         "[%0], [%1], %2, [%3];" ::"r"(dst),
-                         "l"(a.in_re + io), "r"((unsigned)(N * 8)), "r"(mb)
-                         : "memory");
-        } else {
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
-                         "[%0], [%1], %2, [%3];" ::"r"(dst),
-                         "l"(a.in_re + io), "r"((unsigned)(N * 4)), "r"(mb)
-                         : "memory");
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
-                         "[%0], [%1], %2, [%3];" ::"r"(dst + N * 4u),
-                         "l"(a.in_im + io), "r"((unsigned)(N * 4)), "r"(mb)
-                         : "memory");
-        }
+        copy(dst, p0 - h0 / 4, n0, mb);
+        if (!a.interleaved) copy(dst + 4u * kPl, p1 - h1 / 4, n1, mb);
         issued++;
     }
     // Every thread of the group: the current transform has landed.
@@ -101,8 +119,11 @@ struct Lander {
         for (int i = 0; i < fafct::kRingSpin; i++)
             if (fafct::mbar_test(&ctl->bar[g], (unsigned)((issued - 1) & 1))) break;
     }
-    __device__ __forceinline__ LandSrc src(const C2CArgs& a) const {
-        return LandSrc{land, N, a.interleaved, a.sgn};
+    // Transform b (one that landed here) as the first stage's source.
+    __device__ __forceinline__ LandSrc src(const C2CArgs& a, long long b) const {
+        const unsigned h0 = head_bytes(plane(a, b, 0)) / 4;
+        const unsigned h1 = a.interleaved ? 0u : head_bytes(plane(a, b, 1)) / 4;
+        return LandSrc{land + h0, land + kPl + h1, a.interleaved, a.sgn};
     }
 };
 

@@ -317,14 +317,14 @@ static bool ring_ok(const float* x, long long dist) {
     return ((unsigned long long)(size_t)x % 16 == 0) && (dist % 4 == 0);
 }
 
-// Bulk copies of a C2C input into the workspace (k2_c2c_land, power-of-two
-// lengths >= 1024): plane starts 16-byte aligned at every transform.
-static bool land_ok(const float* re, const float* im, long long dist, bool inter) {
+// Bulk copies of a C2C input into the workspace (k2_c2c_land and the
+// tensor-core kernels): any plane alignment and distance; interleaved pairs
+// 8-byte aligned (as the direct loads need).  FAF_CUDA_NO_STAGING=1: direct
+// loads.
+bool land_ok(const float* re, bool inter) {
     const char* env = std::getenv("FAF_CUDA_NO_STAGING");
     if (env && env[0] == '1') return false;
-    if ((unsigned long long)(size_t)re % 16) return false;
-    if (inter) return (2 * dist) % 4 == 0;
-    return (unsigned long long)(size_t)im % 16 == 0 && dist % 4 == 0;
+    return !inter || (unsigned long long)(size_t)re % 8 == 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1000,8 +1000,7 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         // landing from 1024 points (the tensor-core kernels: radix 64 from
         // 4096, radix 16 from 8192)
         const int land_min = p->tc ? (p->d_tc64 ? 12 : 13) : 10;
-        a.land = (p->inner.ct_log2 >= land_min && !window &&
-                  land_ok(in_re, in_im, in_dist, interleaved)) ? 1 : 0;
+        a.land = (p->inner.ct_log2 >= land_min && !window && land_ok(in_re, interleaved)) ? 1 : 0;
         a.err = p->d_wait_err;
         const int slots = p->inner.n;
         if (p->tc) return tc_launch(p, a, st);
@@ -1312,7 +1311,13 @@ static fafk::Geometry geometry64(const FftSize& s, int slots, long long batch) {
     fafk::Geometry g;
     g.E = 16;
     const size_t per = (size_t)2 * plane_floats(slots) * sizeof(double);
-    int G = std::max(1, kThreads64 / s.T);
+    // One transform per CTA from 64 threads up: the engine's barriers are
+    // CTA-wide, so CTAs of one transform progress independently and overlap
+    // each other's loads (B200, 4096 points: 2444 -> 2789 GB/s; 1024: 2729 ->
+    // 3437).  FAF_CUDA_FP64_GROUPS=g: at most g transforms per CTA.
+    int G = std::max(1, std::min(kThreads64, 64) / s.T);
+    if (const char* env = std::getenv("FAF_CUDA_FP64_GROUPS"))
+        G = std::min(std::max(1, kThreads64 / s.T), std::max(1, atoi(env)));
     G = (int)std::min<long long>(G, std::max(1LL, batch));
     while (G > 1 && (size_t)G * per > kMaxSmem) G--;
     g.G = G;

@@ -152,6 +152,9 @@ int c2c_launches(const DevicePlan* p, long long batch);
 // The tensor-core form of a C2C plan (p->tc): kernel attributes (before any
 // capture), and one batched launch (radix 64 where p->d_tc64, else radix 16).
 cudaError_t tc_prepare(const DevicePlan* p);
+// Whether a C2C input may land in shared memory by bulk copy (k2_c2c_land and
+// the tensor-core kernels, power-of-two lengths from 1024).
+bool land_ok(const float* re, bool inter);
 cudaError_t tc_launch(const DevicePlan* p, const fafk::C2CArgs& a, cudaStream_t st);
 
 // Device-pointer executes (enqueue on `st`).

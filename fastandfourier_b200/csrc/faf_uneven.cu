@@ -32,6 +32,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
@@ -488,6 +490,10 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
         a.scale = P.scale;
         a.sgn = u->inverse ? -1.0f : 1.0f;
         a.offs = P.d_offs;
+        // inputs land by bulk copy (k2_c2c_land from 1024 points, the
+        // radix-16 tensor-core kernel from 8192)
+        a.land = (P.log2n >= (P.plan->tc ? 13 : 10) && fafp::land_ok(b.in_re, false)) ? 1 : 0;
+        a.err = P.plan->d_wait_err;
         e = P.plan->tc ? fafp::tc_launch(P.plan, a, ss)
                        : fafk::launch_pot2(0, P.log2n, P.tws, &a, P.g, ss);
         if (e != cudaSuccess) return e;
@@ -630,8 +636,10 @@ extern "C" faf_uneven* faf_uneven_create(const size_t* lengths, size_t count,
         // The graph runs this class beside the other classes' branch.  The
         // radix-64 tensor-core kernel takes all of an SM's shared memory
         // (227 KB), so it would wait for SMs the other branch holds; the
-        // class takes the radix-16 kernel (143 KB) instead.
-        if (p->d_tc64) {
+        // class takes the radix-16 kernel (143 KB) instead, unless
+        // FAF_CUDA_TC_RADIX=64 asks for radix 64.
+        const char* radix = std::getenv("FAF_CUDA_TC_RADIX");
+        if (p->d_tc64 && !(radix && std::strcmp(radix, "64") == 0)) {
             cudaFree(p->d_tc64);
             p->d_tc64 = nullptr;
         }

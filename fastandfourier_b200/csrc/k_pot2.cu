@@ -116,8 +116,9 @@ __global__ void __launch_bounds__(1024) k2_c2c_land(const float2* __restrict__ t
     for (; b - q.g < a.batch; b += stride) {  // the same trip count for every group
         const bool live = b < a.batch;
         if (live) L.wait(a, q.t);
-        const long long oo = (live ? b : 0) * a.out_dist * fpe;
-        fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, L.src(a), q.sync);
+        const long long bi = live ? b : 0;
+        const long long oo = (a.offs ? a.offs[bi] : bi * a.out_dist) * fpe;
+        fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, L.src(a, bi), q.sync);
         float xr[16], xi[16];
         const long long bn = b + stride;
         fafct::ct_stage<N, NS - 1, kTw<N>, 0>(

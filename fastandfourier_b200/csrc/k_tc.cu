@@ -305,7 +305,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if constexpr (LAND) {
             if (live) L.wait(a, q.t);
             const long long bn = b + (long long)gridDim.x * G;
-            tc_run<N, 0, kTw<N>>(xr, xi, q.t, q.ws, q.tw, L.src(a), snk, c, [&]() {
+            tc_run<N, 0, kTw<N>>(xr, xi, q.t, q.ws, q.tw, L.src(a, bi), snk, c, [&]() {
                 __syncthreads();  // every group has read its workspace
                 if (q.t == 0 && bn < a.batch) L.issue(a, bn);
             });

@@ -24,7 +24,7 @@
 // largest magnitude that the row's threads exchange through shared memory.
 //
 // Shared memory (227,360 bytes + the landing control):
-//   [0, 135168)   the workspace: the landed inputs (G x N x 8 bytes), the
+//   [0, 135168)   the workspace: the landed inputs (G x (2 N + 8) floats), the
 //                 A tiles (hi: 2 x 32 KB, lo: 2 x 32 KB), and between the
 //                 stages the intermediate Y[g][kk][b] with rows 66 float2
 //                 apart (so both stages' accesses are free of bank conflicts)
@@ -69,6 +69,7 @@ constexpr uint32_t kOffBar = kOffScB + 256 * 4;    // 2 mbarriers, then the TMEM
 constexpr uint32_t kSmem = kOffBar + 32;
 static_assert(kTabBytes == 83968, "table layout");
 static_assert(kSmem == 227360, "shared-memory map");
+static_assert(4 * (2 * 4096 + 8) * 4 <= kOffB, "four landed 4096-point inputs fit the workspace");
 
 template <int R0>
 struct Geo {
@@ -179,8 +180,8 @@ __device__ __forceinline__ void wait_stage(uint64_t* bars, uint32_t& phase, int*
     fence_after_sync();
 }
 
-// LAND: each transform's input lands at workspace offset g * N * 8 by bulk
-// copy (faf_land.cuh); the next copy is issued once stage B's MMAs have
+// LAND: each transform's input lands at workspace offset g * (2 N + 8)
+// floats by bulk copy (faf_land.cuh); the next copy is issued once stage B's MMAs have
 // completed, while stage B's results are stored.
 template <int R0, bool LAND>
 __global__ void __launch_bounds__(kThreads, 1)
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = tid / T, tt = tid - g * T;  // stage A: transform slot, thread within it
     const int bA = tt & 63, J = tt >> 6;
-    Lander<N> L{&lctl, g, reinterpret_cast<float*>(sm) + (size_t)g * 2 * N};
+    Lander<N> L{&lctl, g, reinterpret_cast<float*>(sm) + (size_t)g * (2 * N + 8)};
     if constexpr (LAND) L.init(tt);
     for (int i = tid; i < (int)(kTabBytes / 16); i += kThreads)
         reinterpret_cast<uint4*>(sm + kOffB)[i] = gtab[i];
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             float mx;
             if constexpr (LAND) {
                 if (live) L.wait(a, tt);
-                mx = stage_a_in<R0>(xr, xi, L.src(a), bA, J, ta);
+                mx = stage_a_in<R0>(xr, xi, L.src(a, live ? bt : 0), bA, J, ta);
             } else {
                 const long long bi = live ? bt : 0;
                 const long long io = (a.offs ? a.offs[bi] : bi * a.in_dist) * fpe;
@@ -388,7 +389,7 @@ cudaError_t launch_r(const C2CArgs& a, const void* tab, int* err, cudaStream_t s
     const long long groups = (a.batch + G - 1) / G;
     const unsigned grid =
         (unsigned)std::max(1LL, std::min(groups, (long long)fafk::sm_count()));
-    if (a.land && !a.offs && !a.window)
+    if (a.land && !a.window)
         k2_c2c_tc64<R0, true><<<grid, kThreads, kSmem, st>>>(a, (const uint4*)tab, err);
     else
         k2_c2c_tc64<R0, false><<<grid, kThreads, kSmem, st>>>(a, (const uint4*)tab, err);

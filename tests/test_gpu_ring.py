@@ -168,7 +168,8 @@ def test_c2c_landed_inputs_match_direct_loads(cuda, monkeypatch, n, batch, inver
 
 def test_c2c_landed_interleaved_and_unaligned(cuda):
     """Interleaved 16384-point inputs land as one copy per transform; plane
-    distances that are not a multiple of 4 floats take the direct loads."""
+    distances that are not a multiple of 4 floats land from the 16-byte block
+    at or below each plane's start."""
     import fastandfourier_b200 as F
     torch = cuda
     n = 16384
@@ -187,6 +188,40 @@ def test_c2c_landed_interleaved_and_unaligned(cuda):
     got = yr.cpu().numpy().reshape(batch, n) + 1j * yi.cpu().numpy().reshape(batch, n)
     assert rel(got, orc.fp64_c2c(xr, xi)) <= REL_L2_TOL
     assert t.wait_status() == 0
+
+
+@pytest.mark.parametrize("n", [1024, 4096, 16384])
+@pytest.mark.parametrize("shift,extra", [(1, 1), (2, 3), (3, 0), (0, 2)])
+def test_c2c_landed_unaligned_planes_match_direct_loads(cuda, monkeypatch, n, shift, extra):
+    """Planes `shift` floats past a 16-byte boundary and `n + extra` floats
+    apart land from the block at or below each start: bit-identical to the
+    direct loads, and to FP64 within the tolerance."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    batch, dist = 300, n + extra
+    rng = seeded(20 + shift + n)
+    xr = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    xi = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    br = torch.zeros(batch * dist + 8, device="cuda")
+    bi = torch.zeros(batch * dist + 8, device="cuda")
+    br[shift:shift + batch * dist].view(batch, dist)[:, :n] = torch.from_numpy(xr).cuda()
+    bi[3 - shift % 4:3 - shift % 4 + batch * dist].view(batch, dist)[:, :n] = \
+        torch.from_numpy(xi).cuda()
+    ir, ii = br[shift:], bi[3 - shift % 4:]
+
+    def run():
+        yr = torch.empty(batch * n, device="cuda")
+        yi = torch.empty(batch * n, device="cuda")
+        t = F.Transform.fft(n)
+        t.execute_batched(F._buf(yr, yi, n, F.L_SPLIT), F._buf(ir, ii, n, F.L_SPLIT), batch,
+                          in_dist=dist, out_dist=n)
+        assert t.wait_status() == 0
+        return yr.cpu().numpy().reshape(batch, n) + 1j * yi.cpu().numpy().reshape(batch, n)
+
+    got = run()
+    assert rel(got, orc.fp64_c2c(xr, xi)) <= REL_L2_TOL
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    assert np.array_equal(got, run())
 
 
 def test_c2c_landed_inputs_unaligned_outputs(cuda):
