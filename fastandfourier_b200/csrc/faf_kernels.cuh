@@ -96,6 +96,9 @@ struct RealArgs {  // R2C / C2R / pipeline / STFT
     const float* filt;
     long long filt_dist, row_len;
     int filt_rows;
+    // C2R of power-of-two inner lengths >= 512 (no filter rows): each
+    // transform's bins land in its group's workspace by bulk copy
+    int land = 0;
 };
 
 // Input ring slot of a CWT row in the power-of-two C2R kernel (inner length

@@ -38,6 +38,16 @@ struct LandSrc {
     }
 };
 
+// `bytes` (a multiple of 16) from the 16-byte aligned `src` to shared
+// address `dst`, completing on the mbarrier at `mb`.
+__device__ __forceinline__ void land_copy(unsigned dst, const float* src, unsigned bytes,
+                                          unsigned mb) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                 "[%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mb)
+                 : "memory");
+}
+
 struct LandCtl {  // static shared memory of a landing kernel
     uint64_t bar[16];
     int failed;
@@ -71,13 +81,6 @@ struct Lander {
     __device__ __forceinline__ static unsigned head_bytes(const float* p) {
         return (unsigned)(reinterpret_cast<uintptr_t>(p) & 15u);
     }
-    __device__ __forceinline__ static void copy(unsigned dst, const float* src, unsigned bytes,
-                                                unsigned mb) {
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
-                     "[%0], [%1], %2, [%3];" ::"r"(dst),
-                     "l"(src), "r"(bytes), "r"(mb)
-                     : "memory");
-    }
     // Thread 0 of the group: transform b's input into the workspace.
     __device__ __forceinline__ void issue(const C2CArgs& a, long long b) {
         if (*(volatile int*)&ctl->failed) return;
@@ -97,8 +100,8 @@ struct Lander {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
                      "r"(n0 + n1)
                      : "memory");
-        copy(dst, p0 - h0 / 4, n0, mb);
-        if (!a.interleaved) copy(dst + 4u * kPl, p1 - h1 / 4, n1, mb);
+        land_copy(dst, p0 - h0 / 4, n0, mb);
+        if (!a.interleaved) land_copy(dst + 4u * kPl, p1 - h1 / 4, n1, mb);
         issued++;
     }
     // Every thread of the group: the current transform has landed.
@@ -124,6 +127,71 @@ struct Lander {
         const unsigned h0 = head_bytes(plane(a, b, 0)) / 4;
         const unsigned h1 = a.interleaved ? 0u : head_bytes(plane(a, b, 1)) / 4;
         return LandSrc{land + h0, land + kPl + h1, a.interleaved, a.sgn};
+    }
+};
+
+// One group's landing of two planes of `nf` floats each (or one interleaved
+// plane of nf pairs) into its workspace, the second plane `pl` floats after
+// the first; each copied from the 16-byte block at or below its start.  The
+// workspace holds 2 pl floats, pl >= nf + 3 rounded up to a multiple of 4.
+struct LandPlanes {
+    LandCtl* ctl;
+    int g;
+    float* land;
+    int pl;
+    int issued = 0, waited = 0;
+
+    __device__ __forceinline__ void init(int t) {
+        if (t == 0)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
+                             fafct::smem_addr(&ctl->bar[g]))
+                         : "memory");
+        if (threadIdx.x == 0) ctl->failed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __device__ __forceinline__ static unsigned head_bytes(const float* p) {
+        return (unsigned)(reinterpret_cast<uintptr_t>(p) & 15u);
+    }
+    // Thread 0 of the group: planes p0 (and p1, unless null: p0 is then nf
+    // interleaved pairs).
+    __device__ __forceinline__ void issue(const float* p0, const float* p1, int nf) {
+        if (*(volatile int*)&ctl->failed) return;
+        const unsigned mb = fafct::smem_addr(&ctl->bar[g]);
+        const unsigned dst = fafct::smem_addr(land);
+        const unsigned h0 = head_bytes(p0);
+        const unsigned n0 = (h0 + (p1 ? 4u : 8u) * (unsigned)nf + 15u) & ~15u;
+        const unsigned h1 = p1 ? head_bytes(p1) : 0u;
+        const unsigned n1 = p1 ? ((h1 + 4u * (unsigned)nf + 15u) & ~15u) : 0u;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb),
+                     "r"(n0 + n1)
+                     : "memory");
+        land_copy(dst, p0 - h0 / 4, n0, mb);
+        if (p1) land_copy(dst + 4u * (unsigned)pl, p1 - h1 / 4, n1, mb);
+        issued++;
+    }
+    __device__ __forceinline__ void wait(int* err, int t) {
+        for (int i = 0; i < fafct::kRingSpin && !*(volatile int*)&ctl->failed; i++)
+            if (fafct::mbar_test(&ctl->bar[g], (unsigned)(waited & 1))) {
+                waited++;
+                return;
+            }
+        if (t == 0) {
+            *(volatile int*)&ctl->failed = 1;
+            if (err) atomicOr(err, 2);
+        }
+    }
+    __device__ __forceinline__ void drain(int t) {
+        if (t != 0 || issued <= waited) return;
+        for (int i = 0; i < fafct::kRingSpin; i++)
+            if (fafct::mbar_test(&ctl->bar[g], (unsigned)((issued - 1) & 1))) break;
+    }
+    // The landed planes' first elements (p0's pairs when p1 is null).
+    __device__ __forceinline__ const float* first(const float* p0) const {
+        return land + head_bytes(p0) / 4;
+    }
+    __device__ __forceinline__ const float* second(const float* p1) const {
+        return land + pl + head_bytes(p1) / 4;
     }
 };
 

@@ -1080,6 +1080,8 @@ cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, 
     fafk::RealArgs a = real_args(p, batch);
     a.in_a = Xr; a.in_b = Xi; a.out_a = y;
     a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
+    // bins land by bulk copy from inner length 512 (k2_c2r_land)
+    a.land = (!p->large && p->inner.ct_log2 >= 9 && land_ok(Xr, interleaved)) ? 1 : 0;
     return launch_c2r_args(p, a, batch, st);
 }
 

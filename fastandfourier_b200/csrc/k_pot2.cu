@@ -470,6 +470,87 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
     if constexpr (RING) fafct::ring_drain(R);
 }
 
+// C2R of power-of-two inner lengths from 512 points (no filter rows): each
+// transform's bins land in its group's workspace by bulk copy (faf_land.cuh),
+// issued for the group's next transform once the last stage has read the
+// workspace.  The pre-pass reads every bin pair the thread owns into
+// registers before the group writes the workspace.
+template <int N>
+__global__ void __launch_bounds__(1024) k2_c2r_land(const float2* __restrict__ tws,
+                                                    const RealArgs a, int G, bool vec) {
+    extern __shared__ float4 smem4[];
+    constexpr int nc = N, T = P2<N, kRO>::T, NS = P2<N, kRO>::NS;
+    constexpr int MP = (nc / 2 + T) / T;
+    static_assert(NS >= 2 && T >= 32, "a group of whole warps and at least two stages");
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    CtGroup<N, kRO> q(sm, N + 1, tws);
+    __shared__ LandCtl ctl;
+    const SmemC mid{q.ws};
+    const int fpe = a.interleaved ? 2 : 1;
+    LandPlanes L{&ctl, q.g, reinterpret_cast<float*>(q.ws), N + 4};
+    L.init(q.t);
+    __syncthreads();
+    auto plane = [&](long long b, int k) -> const float* {
+        return k == 0 ? a.in_a + b * a.in_dist * fpe
+                      : (a.interleaved ? nullptr : a.in_b + b * a.in_dist * fpe);
+    };
+    const long long stride = (long long)gridDim.x * G;
+    long long b = (long long)blockIdx.x * G + q.g;
+    if (q.t == 0 && b < a.batch) L.issue(plane(b, 0), plane(b, 1), nc + 1);
+    for (; b - q.g < a.batch; b += stride) {  // the same trip count for every group
+        const bool live = b < a.batch;
+        const long long bi = live ? b : 0;
+        if (live) L.wait(a.err, q.t);
+        const float* lr = L.first(plane(bi, 0));
+        const float* li = a.interleaved ? nullptr : L.second(plane(bi, 1));
+        auto get = [&](int k) -> cf {
+            if (a.interleaved) {
+                const float2 u = reinterpret_cast<const float2*>(lr)[k];
+                return cf{u.x, u.y};
+            }
+            return cf{lr[k], li[k]};
+        };
+        cf xk[MP], xn[MP];
+#pragma unroll
+        for (int i = 0; i < MP; i++) {
+            const int k = q.t + i * T;
+            if (k <= nc / 2) {
+                xk[i] = get(k);
+                xn[i] = get(nc - k);
+            }
+        }
+        q.sync();  // the group has read the landed bins
+        if (live) {
+#pragma unroll
+            for (int i = 0; i < MP; i++) {
+                const int k = q.t + i * T;
+                if (k <= nc / 2) {
+                    if (k == 0) {
+                        mid.put(0, cf{xk[i].x + xn[i].x, xk[i].x - xn[i].x});
+                    } else {
+                        cf Zk, Znk;
+                        c2r_pair(xk[i], xn[i], __ldg(&a.stw[k - 1]), Zk, Znk);
+                        if (k != nc - k) mid.put(k, Zk);
+                        mid.put(nc - k, Znk);
+                    }
+                }
+            }
+        }
+        q.sync();
+        fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, SmemCConj{q.ws}, q.sync);
+        float xr[16], xi[16];
+        const long long bn = b + stride;
+        fafct::ct_stage<N, NS - 1, kTw<N, kRO>, kRO>(
+            xr, xi, q.t, q.tw, SmemC{q.ws},
+            fafct::LastC<RealPairSink>{RealPairSink{a.out_a + bi * a.out_dist, a.scale, live, vec}},
+            q.sync, [&]() {
+                q.sync();  // the whole group has read the workspace
+                if (q.t == 0 && bn < a.batch) L.issue(plane(bn, 0), plane(bn, 1), nc + 1);
+            });
+    }
+    L.drain(q.t);
+}
+
 // Per bin pair of the pipeline: post-pass -> ops -> pre-pass, in registers,
 // in place on the workspace.
 template <int N, class Ops>
@@ -660,6 +741,14 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
                                    g.smem, st>>>(tws, a, g.G, vec_ok(a.out_a, a.out_dist),
                                                  g.ring);
         } else {
+            if constexpr (N >= 512) {
+                if (a.land) {
+                    if ((e = prep(k2_c2r_land<N>, g.smem)) != cudaSuccess) return e;
+                    k2_c2r_land<N><<<persistent_grid(k2_c2r_land<N>, g, a.batch), g.threads,
+                                     g.smem, st>>>(tws, a, g.G, vec_ok(a.out_a, a.out_dist));
+                    break;
+                }
+            }
             if ((e = prep(k2_c2r<N, false>, g.smem)) != cudaSuccess) return e;
             k2_c2r<N, false><<<persistent_grid(k2_c2r<N, false>, g, a.batch), g.threads, g.smem,
                                st>>>(tws, a, g.G, vec_ok(a.out_a, a.out_dist), 0);

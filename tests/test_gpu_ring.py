@@ -246,3 +246,63 @@ def test_c2c_landed_inputs_unaligned_outputs(cuda):
     assert np.array_equal(got, ar.cpu().numpy() + 1j * ai.cpu().numpy())
     assert rel(got, orc.fp64_c2c(xr, xi)) <= REL_L2_TOL
     assert t.wait_status() == 0
+
+
+@pytest.mark.parametrize("n", [1024, 4096, 32768])
+@pytest.mark.parametrize("batch", [1, 5, 1187])
+@pytest.mark.parametrize("shift,extra", [(0, 0), (1, 2), (3, 5)])
+def test_c2r_landed_bins_match_direct_loads(cuda, monkeypatch, n, batch, shift, extra):
+    """C2R bins (n/2 + 1 per plane, `n/2 + 1 + extra` apart, planes `shift`
+    floats off a 16-byte boundary) land by bulk copy from the block at or
+    below each plane's start: bit-identical to the direct loads, and equal to
+    FP64 within the tolerance."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    nb = n // 2 + 1
+    dist = nb + extra
+    rng = seeded(30 + n + shift)
+    x = rng.standard_normal((batch, n))
+    X = np.fft.rfft(x, axis=1)
+    br = torch.zeros(batch * dist + 8, device="cuda")
+    bi = torch.zeros(batch * dist + 8, device="cuda")
+    br[shift:shift + batch * dist].view(batch, dist)[:, :nb] = torch.from_numpy(
+        X.real.astype(np.float32)).cuda()
+    bi[(shift + 2) % 4:(shift + 2) % 4 + batch * dist].view(batch, dist)[:, :nb] = \
+        torch.from_numpy(X.imag.astype(np.float32)).cuda()
+    ir, ii = br[shift:], bi[(shift + 2) % 4:]
+
+    def run():
+        y = torch.empty(batch * n, device="cuda")
+        t = F.Transform.rfft(n, inverse=True)
+        t.execute_batched(F._buf(y, None, n, F.L_REAL), F._buf(ir, ii, nb, F.L_HERMITIAN),
+                          batch, in_dist=dist, out_dist=n)
+        assert t.wait_status() == 0
+        return y.cpu().numpy().reshape(batch, n)
+
+    got = run()
+    assert rel(got, x) <= REL_L2_TOL  # the inverse real transform's default 1/n
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    assert np.array_equal(got, run())
+
+
+@pytest.mark.parametrize("n", [1024, 4096])
+def test_c2r_landed_interleaved_bins(cuda, monkeypatch, n):
+    """Interleaved Hermitian input lands as one copy per transform."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    batch, nb = 600, n // 2 + 1
+    rng = seeded(40 + n)
+    x = rng.standard_normal((batch, n))
+    X = np.fft.rfft(x, axis=1)
+    z = torch.from_numpy(np.stack([X.real, X.imag], axis=-1).astype(np.float32)).cuda()
+
+    def run():
+        t = F.Transform.rfft(n, inverse=True, layout=F.L_INTERLEAVED)
+        y = t.c2r(z)
+        assert t.wait_status() == 0
+        return y.cpu().numpy().reshape(batch, n)
+
+    got = run()
+    assert rel(got, x) <= REL_L2_TOL
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    assert np.array_equal(got, run())
