@@ -99,7 +99,18 @@ struct RealArgs {  // R2C / C2R / pipeline / STFT
     // C2R of power-of-two inner lengths >= 512 (no filter rows): each
     // transform's bins land in its group's workspace by bulk copy
     int land = 0;
+    // pipeline with one MUL by a spectrum of all N + 1 bins and an input
+    // ring: the spectrum and the super-twiddles are copied to shared memory
+    // behind the ring slots (pipe_table_bytes(N) of them)
+    int stage_tables = 0;
 };
+
+// Shared-memory bytes of the staged pipeline tables for inner length N: the
+// spectrum's real and imaginary planes (N + 1 floats, each padded to N + 4)
+// and the N / 2 super-twiddles.
+__host__ __device__ constexpr size_t pipe_table_bytes(int N) {
+    return (size_t)2 * (N + 4) * 4 + (size_t)(N / 2) * 8;
+}
 
 // Input ring slot of a CWT row in the power-of-two C2R kernel (inner length
 // N): the signal's interleaved spectrum, N + 1 bins rounded up to N + 2, and

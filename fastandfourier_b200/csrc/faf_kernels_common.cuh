@@ -432,6 +432,15 @@ struct OpsMul1Full {
         return cf{v.x * hr - v.y * hi, fmaf(v.x, hi, v.y * hr)};
     }
 };
+// The same product with the spectrum's planes in shared memory.
+struct OpsMulSmem {
+    const float* hr;
+    const float* hi;
+    __device__ __forceinline__ cf operator()(int k, cf v) const {
+        const float r = hr[k], i = hi[k];
+        return cf{v.x * r - v.y * i, fmaf(v.x, i, v.y * r)};
+    }
+};
 __host__ __device__ inline bool ops_single_mul(const RealArgs& a) {
     return a.nops == 1 && a.ops[0].code == OP_MUL;
 }

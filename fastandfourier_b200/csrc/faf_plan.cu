@@ -1195,11 +1195,17 @@ cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long bat
     // issue, not by its loads; a 2-slot ring gains 2 % over direct loads and
     // 3 or 4 slots lose 3 % (a larger shared carve-out leaves less L1 for
     // the spectrum and super-twiddle tables)
-    if (p->inner.ct_log2)
-        return fafk::launch_pot2(3, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? 2 : 0,
-                                             1024),
-                                 st);
+    if (p->inner.ct_log2) {
+        // a single MUL by a spectrum of every bin: the spectrum and the
+        // super-twiddles go to shared memory behind the ring slots
+        const bool stage = a.nops == 1 && a.ops[0].code == fafk::OP_MUL &&
+                           a.ops[0].m == p->inner.n + 1;
+        fafk::Geometry g =
+            geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? 2 : 0, 1024,
+                        stage ? fafk::pipe_table_bytes(p->inner.n) : 0);
+        a.stage_tables = (stage && g.ring >= 2) ? 1 : 0;
+        return fafk::launch_pot2(3, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
+    }
     return fafk::launch_pipeline(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                                  p->inner.d_tw, a, st);
 }

@@ -187,6 +187,22 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
         c = R.cursor(q.g);
         dnext = R.next_offset(q.g);
     }
+    // staged tables (a single MUL by a spectrum of all N + 1 bins): its
+    // planes and the super-twiddles, copied once per CTA behind the ring
+    bool staged = false;
+    if constexpr (RING && fafct::LastPairs<N, kRO>::ok) {
+        if (a.stage_tables) {
+            float* tab = reinterpret_cast<float*>(ring_base<N, kRO>(sm, G, N + 1) + (size_t)K * N);
+            for (int i = threadIdx.x; i <= N; i += blockDim.x) {
+                tab[i] = __ldg(a.ops[0].hr + i);
+                tab[N + 4 + i] = __ldg(a.ops[0].hi_ + i);
+            }
+            float2* st = reinterpret_cast<float2*>(tab + 2 * (N + 4));
+            for (int i = threadIdx.x; i < N / 2; i += blockDim.x) st[i] = __ldg(a.stw + i);
+            __syncthreads();
+            staged = true;
+        }
+    }
     bool first = true;
     CT_FOR_GROUPS(G, a.batch) {
         if constexpr (RING) {
@@ -582,7 +598,8 @@ __device__ __forceinline__ void pipe_middle(int t, const SmemC& mid,
 // (fafct::ct_last_pairs): each thread transforms the bins it owns in
 // registers and writes the pre-pass result back to those same slots.
 // pair_ops serves the bins of the pairs (1 .. N - 1), ops DC and Nyquist.
-template <int N, int SEL = -1, class Ops, class PairOps = Ops>
+// STW_SMEM: the super-twiddles are in shared memory (staged tables).
+template <int N, int SEL = -1, bool STW_SMEM = false, class Ops, class PairOps = Ops>
 __device__ __forceinline__ void pipe_middle_fused(int t, float2* ws, const float2* tw,
                                                   const float2* __restrict__ stw, const Ops& ops,
                                                   const PairOps& pair_ops) {
@@ -595,7 +612,7 @@ __device__ __forceinline__ void pipe_middle_fused(int t, float2* ws, const float
             mid.put(0, cf{x0.x + xn.x, x0.x - xn.x});
         },
         [&](int k, cf zk, cf zn) {
-            const float2 w = __ldg(&stw[k - 1]);
+            const float2 w = STW_SMEM ? stw[k - 1] : __ldg(&stw[k - 1]);
             cf Xk, Xnk;
             r2c_pair(zk, zn, w, Xk, Xnk);
             if (k == N - k) Xk = Xnk;
@@ -626,6 +643,22 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
         c = R.cursor(q.g);
         dnext = R.next_offset(q.g);
     }
+    // staged tables (a single MUL by a spectrum of all N + 1 bins): its
+    // planes and the super-twiddles, copied once per CTA behind the ring
+    bool staged = false;
+    if constexpr (RING && fafct::LastPairs<N, kRO>::ok) {
+        if (a.stage_tables) {
+            float* tab = reinterpret_cast<float*>(ring_base<N, kRO>(sm, G, N + 1) + (size_t)K * N);
+            for (int i = threadIdx.x; i <= N; i += blockDim.x) {
+                tab[i] = __ldg(a.ops[0].hr + i);
+                tab[N + 4 + i] = __ldg(a.ops[0].hi_ + i);
+            }
+            float2* st = reinterpret_cast<float2*>(tab + 2 * (N + 4));
+            for (int i = threadIdx.x; i < N / 2; i += blockDim.x) st[i] = __ldg(a.stw + i);
+            __syncthreads();
+            staged = true;
+        }
+    }
     bool first = true;
     CT_FOR_GROUPS(G, a.batch) {
         if constexpr (RING) {
@@ -649,7 +682,16 @@ __global__ void __launch_bounds__(1024) k2_pipeline(const float2* __restrict__ t
             // a single MUL by a spectrum bound over every bin: no guard on the
             // pairs' bins (mul_bin's guards only act on DC and Nyquist there);
             // any other program (a shorter spectrum included) runs the op loop
-            if (ops_single_mul(a) && a.ops[0].m == N + 1)
+            // (the ring kernel's host always stages that case's tables)
+            if (RING && staged) {
+                // the real plane, then the imaginary one, then the super-twiddles
+                const float* tab =
+                    reinterpret_cast<const float*>(ring_base<N, kRO>(sm, G, N + 1) + (size_t)K * N);
+                pipe_middle_fused<N, kR2cSel<N, RING>, true>(
+                    q.t, q.ws, q.tw, reinterpret_cast<const float2*>(tab + 2 * (N + 4)),
+                    OpsMul1{&a.ops[0]}, OpsMulSmem{tab, tab + N + 4});
+            }
+            else if (!RING && ops_single_mul(a) && a.ops[0].m == N + 1)
                 pipe_middle_fused<N, kR2cSel<N, RING>>(q.t, q.ws, q.tw, a.stw, OpsMul1{&a.ops[0]},
                                                        OpsMul1Full{&a.ops[0]});
             else
