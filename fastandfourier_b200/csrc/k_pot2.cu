@@ -187,22 +187,6 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
         c = R.cursor(q.g);
         dnext = R.next_offset(q.g);
     }
-    // staged tables (a single MUL by a spectrum of all N + 1 bins): its
-    // planes and the super-twiddles, copied once per CTA behind the ring
-    bool staged = false;
-    if constexpr (RING && fafct::LastPairs<N, kRO>::ok) {
-        if (a.stage_tables) {
-            float* tab = reinterpret_cast<float*>(ring_base<N, kRO>(sm, G, N + 1) + (size_t)K * N);
-            for (int i = threadIdx.x; i <= N; i += blockDim.x) {
-                tab[i] = __ldg(a.ops[0].hr + i);
-                tab[N + 4 + i] = __ldg(a.ops[0].hi_ + i);
-            }
-            float2* st = reinterpret_cast<float2*>(tab + 2 * (N + 4));
-            for (int i = threadIdx.x; i < N / 2; i += blockDim.x) st[i] = __ldg(a.stw + i);
-            __syncthreads();
-            staged = true;
-        }
-    }
     bool first = true;
     CT_FOR_GROUPS(G, a.batch) {
         if constexpr (RING) {
