@@ -227,7 +227,10 @@ bool large_pot2_supported(int n1, int n2);
 long long large_pot2_chunk(long long n);       // transforms per scratch chunk
 int large_pot2_launches(int n1, int n2, long long batch);
 cudaError_t large_pot2_prepare(int n1, int n2);  // kernel attributes + module, before any capture
-cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st);
+// `threads` per CTA of both passes: 256, 512 or 1024; 0 = the default of a
+// standalone batch (FAF_CUDA_4STEP_THREADS overrides both).
+cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st,
+                              int threads = 0);
 
 // FP64 transforms (k_fp64.cu): kind 0 = C2C (C2C64Args), 1 = R2C, 2 = C2R
 // (Real64Args), on the FP64 runtime-radix engine, at most 512 threads per CTA.

@@ -469,7 +469,9 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
             a2.tws1 = L.plan->f1.d_tws; a2.tws2 = L.plan->f2.d_tws; a2.twm = L.plan->d_tw_big;
             a2.scratch = u->d_scratch;
             a2.scratch_transforms = fafk::large_pot2_chunk((long long)L.la.n1 * L.la.n2);
-            if ((e = fafk::launch_large_pot2(L.la.n1, L.la.n2, a2, st)) != cudaSuccess) return e;
+            // 512 threads per CTA: two CTAs per SM leave the other branch room
+            if ((e = fafk::launch_large_pot2(L.la.n1, L.la.n2, a2, st, 512)) != cudaSuccess)
+                return e;
             continue;
         }
         fafk::LargeArgs la = L.la;

@@ -150,14 +150,18 @@ __global__ void __launch_bounds__(TH, 1024 / TH)
     }
 }
 
-// Threads per CTA of both passes: 512, two CTAs per SM (FAF_CUDA_4STEP_THREADS
-// =1024: one CTA of 1024).  Measured on B200: 65536-point C2C, batch 512,
-// 1636 -> 1907 GB/s; 32768, batch 1024, 1528 -> 1775; the uneven graph
-// 1651 -> 1777.  The two CTAs of an SM drift apart, so one loads its columns
-// while the other computes.
-inline int cta_threads() {
+// Threads per CTA of both passes.  The CTAs of an SM drift apart, so some
+// load their columns while others compute.  Measured on B200 (65536-point
+// C2C, batch 512 / 32768, batch 1024 / the uneven graph), in GB/s:
+//   one CTA of 1024:   1636 / 1528 / 1651
+//   two CTAs of 512:   1900 / 1786 / 1872
+//   four CTAs of 256:  2044 / 1986 / 1767
+// A standalone batch takes 256; the uneven graph, whose other branch needs
+// SMs of its own, takes 512 (`want`).  FAF_CUDA_4STEP_THREADS overrides both.
+inline int cta_threads(int want) {
     const char* e = std::getenv("FAF_CUDA_4STEP_THREADS");
-    return (e && atoi(e) == 1024) ? 1024 : 512;
+    const int v = e ? atoi(e) : (want ? want : 256);
+    return (v == 1024 || v == 512) ? v : 256;
 }
 
 // Kernel attributes (dynamic shared memory above 48 KB), set once per
@@ -202,15 +206,19 @@ cudaError_t launch_pair_t(const Large2Args& a, cudaStream_t st) {
 }
 
 template <int N1, int N2>
-cudaError_t launch_pair(const Large2Args& a, cudaStream_t st) {
-    return cta_threads() == 512 ? launch_pair_t<N1, N2, 512>(a, st)
-                                : launch_pair_t<N1, N2, 1024>(a, st);
+cudaError_t launch_pair(const Large2Args& a, cudaStream_t st, int want) {
+    switch (cta_threads(want)) {
+    case 1024: return launch_pair_t<N1, N2, 1024>(a, st);
+    case 256: return launch_pair_t<N1, N2, 256>(a, st);
+    default: return launch_pair_t<N1, N2, 512>(a, st);
+    }
 }
 
 template <int N1, int N2>
 cudaError_t load_both() {
     cudaError_t e = load_pair<N1, N2, 1024>();
-    return e == cudaSuccess ? load_pair<N1, N2, 512>() : e;
+    if (e == cudaSuccess) e = load_pair<N1, N2, 512>();
+    return e == cudaSuccess ? load_pair<N1, N2, 256>() : e;
 }
 
 }  // namespace l2p
@@ -235,11 +243,12 @@ cudaError_t large_pot2_prepare(int n1, int n2) {
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st) {
+cudaError_t launch_large_pot2(int n1, int n2, const Large2Args& a, cudaStream_t st,
+                              int threads) {
     if (a.batch <= 0) return cudaSuccess;
-    if (n1 == 128 && n2 == 128) return l2p::launch_pair<128, 128>(a, st);
-    if (n1 == 128 && n2 == 256) return l2p::launch_pair<128, 256>(a, st);
-    if (n1 == 256 && n2 == 256) return l2p::launch_pair<256, 256>(a, st);
+    if (n1 == 128 && n2 == 128) return l2p::launch_pair<128, 128>(a, st, threads);
+    if (n1 == 128 && n2 == 256) return l2p::launch_pair<128, 256>(a, st, threads);
+    if (n1 == 256 && n2 == 256) return l2p::launch_pair<256, 256>(a, st, threads);
     return cudaErrorInvalidValue;
 }
 

@@ -467,17 +467,19 @@ def test_c2c_16384_two_pass_four_step(cuda, monkeypatch, inverse):
 
 
 @pytest.mark.parametrize("n", [32768, 65536])
-def test_four_step_cta_widths_agree(cuda, monkeypatch, n):
-    """The two-pass four-step gives the same values with 512- and 1024-thread
-    CTAs (each column and row runs the same arithmetic)."""
+@pytest.mark.parametrize("threads", ["512", "1024"])
+def test_four_step_cta_widths_agree(cuda, monkeypatch, n, threads):
+    """The two-pass four-step gives the same values with CTAs of 256 (the
+    standalone default), 512 (the uneven graph's) and 1024 threads: each
+    column and row runs the same arithmetic."""
     import fastandfourier_b200 as F
     torch = cuda
     rng = seeded(n)
-    re = rng.uniform(-1, 1, (5, n)).astype(np.float32)
-    im = rng.uniform(-1, 1, (5, n)).astype(np.float32)
+    re = rng.uniform(-1, 1, (150, n)).astype(np.float32)
+    im = rng.uniform(-1, 1, (150, n)).astype(np.float32)
     t = F.Transform.fft(n)
     ar, ai = t.c2c(dev(torch, re), dev(torch, im))
-    monkeypatch.setenv("FAF_CUDA_4STEP_THREADS", "1024")
+    monkeypatch.setenv("FAF_CUDA_4STEP_THREADS", threads)
     br, bi = t.c2c(dev(torch, re), dev(torch, im))
     assert torch.equal(ar, br) and torch.equal(ai, bi)
     assert orc.rel_l2_complex(host(ar), host(ai), orc.fp64_c2c(re, im)) <= REL_L2_TOL
