@@ -403,8 +403,11 @@ def gpu_lead(torch, stream):
     timed region opened after it starts with work already queued behind it:
     the host's call for the first timed step then runs while the GPU spins,
     not inside the timed region.  Nothing of a timed step is skipped."""
+    sleep = getattr(torch.cuda, "_sleep", None)
+    if sleep is None:  # no spin available: the timed region opens on an idle GPU
+        return
     with torch.cuda.stream(stream):
-        torch.cuda._sleep(1_000_000)
+        sleep(1_000_000)
 
 
 def time_steps(torch, stream, steps, fn):
