@@ -34,7 +34,8 @@ extern "C" {
 /* 1 if a CUDA device is usable, 0 otherwise (message in faf_get_error()). */
 int faf_cuda_available(void);
 /* Name of the plan kind behind t ("c2c", "rader", "bluestein", "r2c", "c2r",
- * "pipeline", "stft", "c2c-4step", ...), or NULL. */
+ * "pipeline", "stft", "c2c-4step", the tensor-core forms "c2c-tc" (radix-16
+ * stages) and "c2c-tc64" (64-point DFTs), ...), or NULL. */
 const char *faf_cuda_plan_kind(const faf_transform *t);
 /* Tensor-core plans: 0 if every MMA wait of this plan's launches so far
  * completed, 1 if one ran out of its bound (the results are then invalid);
