@@ -10,7 +10,7 @@ once, each output sample written once: 8 bytes per sample) and its fraction
 of the measured HBM copy bandwidth.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload pipeline|r2c|c2c1024|c2c16384|c2c16384tc|c2c4096fp64|
+                    [--workload pipeline|r2c|c2c1024|c2c4096|c2c16384|c2c16384tc|c2c4096fp64|
                                 stft|istft|cwt|icwt|uneven|serve]
 
 --workload serve replays a Poisson request trace (20k requests/s: 40% rfft
@@ -69,6 +69,8 @@ WORKLOADS = {
                 16 * 1024, 5 * 1024 * 10),
     "c2c16384": ("C2C n=16384 batch 2048 forward (split planes), seed 3", 16384, 2048,
                  16 * 16384, 5 * 16384 * 14),
+    "c2c4096": ("C2C n=4096 batch 8192 forward (split planes, inputs landed by bulk copy), seed 3",
+                4096, 8192, 16 * 4096, 5 * 4096 * 12),
     "c2c16384tc": ("C2C n=16384 batch 2048 forward, tensor-core form (64-point DFTs as FP16 "
                    "hi+lo tcgen05 MMAs in two passes, radix-4 on CUDA cores, FP32 accumulation), "
                    "seed 3, 1% of entries x1e3",
@@ -627,7 +629,8 @@ def run_ours(args, rank, world, local_rank):
                 "kernel": {"pipeline": "k2_pipeline", "r2c": "k2_r2c", "stft": "k2_stft",
                            "uneven": "k4p_col (65536-point class, column pass; traffic of one "
                                      "128-transform chunk)",
-                           "c2c16384": "k2_c2c_land", "c2c16384tc": "k2_c2c_tc64",
+                           "c2c16384": "k2_c2c_land", "c2c4096": "k2_c2c_land",
+                           "c2c16384tc": "k2_c2c_tc64",
                            "c2c4096fp64": "k64_c2c", "istft": "k2_c2r + k_ola",
                            "cwt": "k2_c2r (bank rows) + k2_r2c",
                            "icwt": "k2_r2c (rows) + k_icwt_acc + k2_c2r"}.get(
