@@ -160,7 +160,8 @@ __device__ __forceinline__ void ct_r2c_post(int t, const SmemC& mid,
 // 4641 to 5007 GB/s (no spills), the pipeline from 2369 to 2432 GB/s (despite
 // 40 bytes of spills); with the unguarded multiply of a full-length spectrum,
 // 2691 against 2638 GB/s for a branch of its own (136 against 44 bytes of
-// spills).  Elsewhere the default (selects only for one-warp
+// spills), and with that spectrum staged in shared memory 2822 against 2657
+// (84 against 48 bytes).  Elsewhere the default (selects only for one-warp
 // transforms): the selects spill more at other lengths and in the direct-load
 // kernels.
 template <int N, bool RING>
