@@ -194,7 +194,11 @@ cudaError_t launch_pair_t(const Large2Args& a, cudaStream_t st) {
     cudaError_t e = prepare_pair<N1, N2, TH>();
     if (e != cudaSuccess) return e;
     const int sms = fafk::sm_count();
-    const long long chunk = std::max(1LL, a.scratch_transforms);
+    // chunks of equal size (at most scratch_transforms each), so that no
+    // chunk is a short tail that fills only part of the GPU
+    const long long cap = std::max(1LL, a.scratch_transforms);
+    const long long nch = (a.batch + cap - 1) / cap;
+    const long long chunk = (a.batch + nch - 1) / nch;
     for (long long b0 = 0; b0 < a.batch; b0 += chunk) {
         const long long nb = std::min(chunk, a.batch - b0);
         const long long t1 = nb * (N2 / Cols<N1, TH>::W), t2 = nb * (N1 / Cols<N2, TH>::W);
