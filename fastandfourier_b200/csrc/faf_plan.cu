@@ -300,13 +300,17 @@ fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long
     return g;
 }
 
-// Input ring slots of the STFT kernel (FAF_CUDA_STFT_RING overrides).
-// Measured on B200 (Hann 1024 / hop 256, 64 x 2^18 samples): 4 slots 129.5
-// us, 8 slots 131.4, 2 slots 171.7, direct loads 137.0.
+// Input ring slots and CTA width of the STFT kernel (FAF_CUDA_STFT_RING and
+// FAF_CUDA_CTA_THREADS override).  Measured on B200 (Hann 1024 / hop 256,
+// 64 x 2^18 samples, 200-step event loops): 384 threads (12 groups) with 8
+// slots 105.6 us; 512 threads (15 groups) with 8 slots 106.7, with 4 slots
+// 118.9; 256 threads with 6 slots 106.8.  With 4 slots behind 12 or 15
+// groups, groups wait for a free slot.
 static int stft_ring() {
     const char* env = std::getenv("FAF_CUDA_STFT_RING");
-    return env ? atoi(env) : 4;
+    return env ? atoi(env) : 8;
 }
+constexpr int kStftThreads = 384;
 
 // Bulk copies of a real input into the ring need every transform start
 // 16-byte aligned: base address and distance (floats) a multiple of 4.
@@ -1226,7 +1230,7 @@ cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long 
     if (p->inner.ct_log2)
         return fafk::launch_pot2(
             4, p->inner.ct_log2, p->inner.d_tws, &a,
-            geometry_ct(p->inner, slots, batch, ring ? stft_ring() : 0, 512,
+            geometry_ct(p->inner, slots, batch, ring ? stft_ring() : 0, kStftThreads,
                         ((size_t)a.win * sizeof(float) + 15) & ~(size_t)15),
             st);
     return fafk::launch_stft(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
