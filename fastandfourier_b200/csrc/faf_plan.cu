@@ -242,11 +242,23 @@ void free_size(FftSize& s) {
 
 // Geometry of the compile-time kernels: interleaved float2 workspace with one
 // pad element per 16 (plane2), T = n / 16 threads per transform, about
-// `target_threads` threads per CTA.  With ring > 0 (and n >= 512), the shared
+// `target_threads` threads per CTA (0: by length, below).  With ring > 0 (and n >= 512), the shared
 // memory left after the workspaces holds up to `ring` input ring slots (n
 // float2 each, at most fafct::kRingMax) and `ring_extra` bytes behind them;
 // fewer than 2 slots means no ring.
 static int device_sms() { return fafk::sm_count(); }
+
+// Default CTA width of the C2C and C2R kernels by inner length.  Measured on
+// B200 (2^25 points per launch, 50-launch event loops, GB/s at 256 / 512 /
+// 1024 threads): C2C 512 2941 / 2803 / 2803, 2048 5340 / 5432 / 5581, 4096
+// 4585 / 4876 / 5116, 8192 3608 / 3606 / 3854; C2R (inner length n / 2)
+// 1024 4246 / 4136 / 4137, 4096 3758 / 3891 / 4195, 8192 3407 / 3493 / 3763,
+// 16384 2974 / 2972 / 3190.  Other lengths differ by < 2 %.
+static int default_threads(int ct_log2) {
+    if (ct_log2 >= 11) return 1024;
+    if (ct_log2 == 9) return 256;
+    return 512;
+}
 
 fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int ring,
                            int target_threads, size_t ring_extra, size_t slot_bytes) {
@@ -257,7 +269,7 @@ fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int rin
     const int plane2 = (slots - 1) + ((slots - 1) >> 4) + 1;
     const size_t table = fafk::pot2_table_smem(s.ct_log2, s.ct_ord);
     const size_t per = (size_t)((plane2 + 1) & ~1) * sizeof(float2);
-    int target = target_threads;
+    int target = target_threads > 0 ? target_threads : default_threads(s.ct_log2);
     if (const char* env = std::getenv("FAF_CUDA_CTA_THREADS")) target = std::max(1, atoi(env));
     int G = std::max(1, target / T);
     // a small batch spreads over every SM (one transform per group, as many

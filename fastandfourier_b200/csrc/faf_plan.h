@@ -42,7 +42,7 @@ void free_size(FftSize& s);
 int plane_floats(int slots);
 fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long batch);
 fafk::Geometry geometry_ct(const FftSize& s, int slots, long long batch, int ring = 0,
-                           int target_threads = 512, size_t ring_extra = 0,
+                           int target_threads = 0, size_t ring_extra = 0,
                            size_t slot_bytes = 0);
 
 enum class Kind {
