@@ -312,6 +312,37 @@ fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long
     return g;
 }
 
+// CTA width and input-ring slots of the R2C and pipeline kernels by inner
+// length (2^ct_log2).  Measured on B200 (2^25 samples per launch, 40-launch
+// event loops, GB/s):
+//   R2C n = 256 / 512: 256 threads 3245 / 3582, 1024 threads 2857 / 3377
+//     (no ring below inner length 512); n = 2048: 256 threads with 2 slots
+//     4848, 1024 threads with 8 slots 4486; n = 4096 and up: 1024 threads
+//     with 8 slots (5012 at 4096; 256 or 512 threads 3200-4420).
+//   pipeline n = 512: 512 threads 2806, 1024 2552; n = 1024: 1024 threads
+//     with 4 slots 2751, with 2 slots 2458; n = 2048: 512 threads with 3
+//     slots 2691, 1024 threads with 2 slots 2239; n = 4096 (200-step bench
+//     line): 1024 threads with 3 slots 2845, with 2 slots 2821-2829.  From
+//     n = 8192 no ring fits beside 1024 threads' workspaces and the staged
+//     tables, and the unstaged kernel at 1024 threads is the fastest (1974
+//     against 1449 with 512 threads, ring and staged tables).
+struct RealShape {
+    int threads, ring;
+};
+static RealShape r2c_shape(int ct_log2) {
+    if (ct_log2 == 7 || ct_log2 == 8 || ct_log2 == 10) return {256, 2};
+    return {1024, fafct::kRingMax};
+}
+static RealShape pipe_shape(int ct_log2) {
+    switch (ct_log2) {
+    case 8: return {512, 2};
+    case 9: return {1024, 4};
+    case 10: return {512, 3};
+    case 11: return {1024, 3};
+    default: return {1024, 2};
+    }
+}
+
 // Input ring slots and CTA width of the STFT kernel (FAF_CUDA_STFT_RING and
 // FAF_CUDA_CTA_THREADS override).  Measured on B200 (Hann 1024 / hop 256,
 // 64 x 2^18 samples, 200-step event loops): 384 threads (12 groups) with 8
@@ -1065,14 +1096,13 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
         return run_large(p, 1, &a, batch, st);
     }
     const int slots = p->inner.n + 1;
-    // measured on B200 (n = 4096, batch 8192): 8 groups of 128 threads with
-    // a 4-slot input ring (as many slots as fit), 61 us per launch against 70
-    // with direct loads
-    if (p->inner.ct_log2)
+    if (p->inner.ct_log2) {
+        const RealShape sh = r2c_shape(p->inner.ct_log2);
         return fafk::launch_pot2(
             1, p->inner.ct_log2, p->inner.d_tws, &a,
-            geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? fafct::kRingMax : 0, 1024),
+            geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? sh.ring : 0, sh.threads),
             st);
+    }
     return fafk::launch_r2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);
 }
@@ -1207,17 +1237,14 @@ cudaError_t exec_pipeline(DevicePlan* p, const float* x, float* y, long long bat
         return run_large(p, 3, &a, batch, st);
     }
     const int slots = p->inner.n + 1;
-    // measured on B200 (n = 4096, batch 8192): the two-FFT kernel is bound by
-    // issue, not by its loads; a 2-slot ring gains 2 % over direct loads and
-    // 3 or 4 slots lose 3 % (a larger shared carve-out leaves less L1 for
-    // the spectrum and super-twiddle tables)
     if (p->inner.ct_log2) {
+        const RealShape sh = pipe_shape(p->inner.ct_log2);
         // a single MUL by a spectrum of every bin: the spectrum and the
         // super-twiddles go to shared memory behind the ring slots
         const bool stage = a.nops == 1 && a.ops[0].code == fafk::OP_MUL &&
                            a.ops[0].m == p->inner.n + 1;
         fafk::Geometry g =
-            geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? 2 : 0, 1024,
+            geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? sh.ring : 0, sh.threads,
                         stage ? fafk::pipe_table_bytes(p->inner.n) : 0);
         a.stage_tables = (stage && g.ring >= 2) ? 1 : 0;
         return fafk::launch_pot2(3, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
