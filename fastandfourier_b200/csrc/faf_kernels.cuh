@@ -64,13 +64,17 @@ struct C2CArgs {
     int interleaved;
     const float* window;  // optional per-sample real window (STFT frame), or NULL
     const long long* offs = nullptr;  // per-transform element offsets (in and out), or NULL
-    // power-of-two lengths >= 1024: each transform's input lands in its
-    // group's workspace by bulk copy (inputs 16-byte aligned, distance a
-    // multiple of 4 floats, no window, no offsets); err records a wait that
-    // ran out
+    // power-of-two lengths >= 64: each transform's input lands in its
+    // group's workspace by bulk copy (any plane alignment, distance and
+    // offset list; interleaved pairs 8-byte aligned; no window); err records
+    // a wait that ran out
     int land = 0;
     int* err = nullptr;
 };
+
+// Groups per CTA of a landing C2C kernel whose transforms are narrower than
+// a warp (one mbarrier each); groups of a warp or more stop at 15.
+constexpr int kLandMaxGroups = 64;
 
 struct RealArgs {  // R2C / C2R / pipeline / STFT
     const float* in_a;    // R2C: x; C2R: X re

@@ -48,18 +48,21 @@ __device__ __forceinline__ void land_copy(unsigned dst, const float* src, unsign
                  : "memory");
 }
 
-struct LandCtl {  // static shared memory of a landing kernel
-    uint64_t bar[16];
+// Static shared memory of a landing kernel: one mbarrier per group.
+template <int MAXG>
+struct LandCtlN {
+    uint64_t bar[MAXG];
     int failed;
 };
+using LandCtl = LandCtlN<16>;
 
 // One group's landing: its mbarrier and workspace.  `issued` is counted by
 // the group's thread 0, `waited` by every thread of the group.  The
 // workspace holds 2 N + 8 floats.
-template <int N>
+template <int N, class Ctl = LandCtl>
 struct Lander {
     static constexpr int kPl = N + 4;  // floats from the landed real plane to the imaginary one
-    LandCtl* ctl;
+    Ctl* ctl;
     int g;
     float* land;
     int issued = 0, waited = 0;

@@ -1044,16 +1044,23 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         a.in_dist = in_dist; a.out_dist = out_dist; a.batch = batch;
         a.scale = p->scale; a.sgn = sgn; a.interleaved = interleaved ? 1 : 0;
         a.window = window;
-        // landing from 1024 points (the tensor-core kernels: radix 64 from
+        // landing from 64 points (the tensor-core kernels: radix 64 from
         // 4096, radix 16 from 8192)
-        const int land_min = p->tc ? (p->d_tc64 ? 12 : 13) : 10;
+        const int land_min = p->tc ? (p->d_tc64 ? 12 : 13) : 6;
         a.land = (p->inner.ct_log2 >= land_min && !window && land_ok(in_re, interleaved)) ? 1 : 0;
         a.err = p->d_wait_err;
         const int slots = p->inner.n;
         if (p->tc) return tc_launch(p, a, st);
-        if (p->inner.ct_log2)
-            return fafk::launch_pot2(0, p->inner.ct_log2, p->inner.d_tws, &a,
-                                     geometry_ct(p->inner, slots, batch), st);
+        if (p->inner.ct_log2) {
+            fafk::Geometry g = geometry_ct(p->inner, slots, batch);
+            // one landing mbarrier per group
+            if (a.land && g.G > fafk::kLandMaxGroups) {
+                g.smem = g.smem / g.G * fafk::kLandMaxGroups;
+                g.G = fafk::kLandMaxGroups;
+                g.threads = g.G * (p->inner.n / 16);
+            }
+            return fafk::launch_pot2(0, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
+        }
         return fafk::launch_c2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                                 p->inner.d_tw, a, st);
     }

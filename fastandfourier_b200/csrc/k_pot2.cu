@@ -92,8 +92,8 @@ __global__ void __launch_bounds__(1024) k2_c2c(const float2* __restrict__ tws, c
     }
 }
 
-// C2C of power-of-two lengths from 1024 points (at most 16 groups, one
-// mbarrier each): the first stage's scalar global loads, with few transforms
+// C2C of power-of-two lengths from 64 points (one mbarrier per group: at
+// most 15 groups of one warp or more, kLandMaxGroups narrower ones): the first stage's scalar global loads, with few transforms
 // per CTA to overlap them with, left the kernel waiting on memory.
 // Here each transform's input lands in its group's workspace by bulk copy
 // (faf_land.cuh), issued for the group's next transform as soon as the last
@@ -104,10 +104,11 @@ __global__ void __launch_bounds__(1024) k2_c2c_land(const float2* __restrict__ t
                                                     const C2CArgs a, int G) {
     extern __shared__ float4 smem4[];
     CtGroup<N> q(reinterpret_cast<float2*>(smem4), N, tws);
-    __shared__ LandCtl ctl;
+    using Ctl = LandCtlN<(P2<N>::T >= 32 ? 16 : kLandMaxGroups)>;
+    __shared__ Ctl ctl;
     constexpr int NS = P2<N>::NS;
     const int fpe = a.interleaved ? 2 : 1;
-    Lander<N> L{&ctl, q.g, reinterpret_cast<float*>(q.ws)};
+    Lander<N, Ctl> L{&ctl, q.g, reinterpret_cast<float*>(q.ws)};
     L.init(q.t);
     __syncthreads();
     const long long stride = (long long)gridDim.x * G;
@@ -735,7 +736,7 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     switch (kind) {
     case 0: {
         const C2CArgs& a = *(const C2CArgs*)args;
-        if constexpr (N >= 1024) {
+        if constexpr (N >= 64) {
             if (a.land) {
                 if ((e = prep(k2_c2c_land<N>, g.smem)) != cudaSuccess) return e;
                 k2_c2c_land<N><<<persistent_grid(k2_c2c_land<N>, g, a.batch), g.threads, g.smem,

@@ -149,11 +149,11 @@ def _c2c_pair(torch, F, n, batch, inverse, inter, seed):
     return re, im, got
 
 
-@pytest.mark.parametrize("n", [1024, 2048, 4096, 8192, 16384])
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024, 2048, 4096, 8192, 16384])
 @pytest.mark.parametrize("batch", [1, 3, 149, 300, 1500])
 @pytest.mark.parametrize("inverse", [False, True])
 def test_c2c_landed_inputs_match_direct_loads(cuda, monkeypatch, n, batch, inverse):
-    """Power-of-two C2C of 1024 to 16384 points lands each transform's planes
+    """Power-of-two C2C of 64 to 16384 points lands each transform's planes
     in the workspace by bulk copy; the result equals the direct loads bit for
     bit (same arithmetic) and FP64 within the tolerance."""
     import fastandfourier_b200 as F
@@ -190,7 +190,21 @@ def test_c2c_landed_interleaved_and_unaligned(cuda):
     assert t.wait_status() == 0
 
 
-@pytest.mark.parametrize("n", [1024, 4096, 16384])
+@pytest.mark.parametrize("n", [64, 128, 512, 1024])
+def test_c2c_landed_interleaved_matches_direct_loads(cuda, monkeypatch, n):
+    """Interleaved inputs of sub-warp, one-warp (512-point) and two-warp
+    transforms land as one copy per transform, bit-identical to the direct
+    loads."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    re, im, got = _c2c_pair(torch, F, n, 1187, False, True, 9)
+    assert rel(got, orc.fp64_c2c(re, im)) <= REL_L2_TOL
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    _, _, direct = _c2c_pair(torch, F, n, 1187, False, True, 9)
+    assert np.array_equal(got, direct)
+
+
+@pytest.mark.parametrize("n", [64, 256, 512, 1024, 4096, 16384])
 @pytest.mark.parametrize("shift,extra", [(1, 1), (2, 3), (3, 0), (0, 2)])
 def test_c2c_landed_unaligned_planes_match_direct_loads(cuda, monkeypatch, n, shift, extra):
     """Planes `shift` floats past a 16-byte boundary and `n + extra` floats
