@@ -137,8 +137,9 @@ struct Lander {
 // plane of nf pairs) into its workspace, the second plane `pl` floats after
 // the first; each copied from the 16-byte block at or below its start.  The
 // workspace holds 2 pl floats, pl >= nf + 3 rounded up to a multiple of 4.
+template <class Ctl = LandCtl>
 struct LandPlanes {
-    LandCtl* ctl;
+    Ctl* ctl;
     int g;
     float* land;
     int pl;

@@ -343,6 +343,15 @@ static RealShape pipe_shape(int ct_log2) {
     }
 }
 
+// A landing kernel has one mbarrier per group: at most kLandMaxGroups groups
+// (groups of a warp or more already stop at 15).  `g` holds workspaces only.
+static void cap_land_groups(fafk::Geometry& g, int T) {
+    if (g.G <= fafk::kLandMaxGroups) return;
+    g.smem = g.smem / g.G * fafk::kLandMaxGroups;
+    g.G = fafk::kLandMaxGroups;
+    g.threads = g.G * T;
+}
+
 // Input ring slots and CTA width of the STFT kernel (FAF_CUDA_STFT_RING and
 // FAF_CUDA_CTA_THREADS override).  Measured on B200 (Hann 1024 / hop 256,
 // 64 x 2^18 samples, 200-step event loops): 384 threads (12 groups) with 8
@@ -1053,12 +1062,7 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         if (p->tc) return tc_launch(p, a, st);
         if (p->inner.ct_log2) {
             fafk::Geometry g = geometry_ct(p->inner, slots, batch);
-            // one landing mbarrier per group
-            if (a.land && g.G > fafk::kLandMaxGroups) {
-                g.smem = g.smem / g.G * fafk::kLandMaxGroups;
-                g.G = fafk::kLandMaxGroups;
-                g.threads = g.G * (p->inner.n / 16);
-            }
+            if (a.land) cap_land_groups(g, p->inner.n / 16);
             return fafk::launch_pot2(0, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
         }
         return fafk::launch_c2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
@@ -1121,9 +1125,11 @@ static cudaError_t launch_c2r_args(DevicePlan* p, fafk::RealArgs& a, long long b
         return run_large(p, 2, &a, batch, st);
     }
     const int slots = p->inner.n + 1;
-    if (p->inner.ct_log2)
-        return fafk::launch_pot2(2, p->inner.ct_log2, p->inner.d_tws, &a,
-                                 geometry_ct(p->inner, slots, batch), st);
+    if (p->inner.ct_log2) {
+        fafk::Geometry g = geometry_ct(p->inner, slots, batch);
+        if (a.land) cap_land_groups(g, p->inner.n / 16);
+        return fafk::launch_pot2(2, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
+    }
     return fafk::launch_c2r(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);
 }
@@ -1133,8 +1139,8 @@ cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, 
     fafk::RealArgs a = real_args(p, batch);
     a.in_a = Xr; a.in_b = Xi; a.out_a = y;
     a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
-    // bins land by bulk copy from inner length 512 (k2_c2r_land)
-    a.land = (!p->large && p->inner.ct_log2 >= 9 && land_ok(Xr, interleaved)) ? 1 : 0;
+    // bins land by bulk copy from inner length 64 (k2_c2r_land)
+    a.land = (!p->large && p->inner.ct_log2 >= 6 && land_ok(Xr, interleaved)) ? 1 : 0;
     return launch_c2r_args(p, a, batch, st);
 }
 

@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
     if constexpr (RING) fafct::ring_drain(R);
 }
 
-// C2R of power-of-two inner lengths from 512 points (no filter rows): each
+// C2R of power-of-two inner lengths from 64 points (no filter rows): each
 // transform's bins land in its group's workspace by bulk copy (faf_land.cuh),
 // issued for the group's next transform once the last stage has read the
 // workspace.  The pre-pass reads every bin pair the thread owns into
@@ -483,13 +483,14 @@ __global__ void __launch_bounds__(1024) k2_c2r_land(const float2* __restrict__ t
     extern __shared__ float4 smem4[];
     constexpr int nc = N, T = P2<N, kRO>::T, NS = P2<N, kRO>::NS;
     constexpr int MP = (nc / 2 + T) / T;
-    static_assert(NS >= 2 && T >= 32, "a group of whole warps and at least two stages");
+    static_assert(NS >= 2, "at least two stages");
     float2* sm = reinterpret_cast<float2*>(smem4);
     CtGroup<N, kRO> q(sm, N + 1, tws);
-    __shared__ LandCtl ctl;
+    using Ctl = LandCtlN<(T >= 32 ? 16 : kLandMaxGroups)>;
+    __shared__ Ctl ctl;
     const SmemC mid{q.ws};
     const int fpe = a.interleaved ? 2 : 1;
-    LandPlanes L{&ctl, q.g, reinterpret_cast<float*>(q.ws), N + 4};
+    LandPlanes<Ctl> L{&ctl, q.g, reinterpret_cast<float*>(q.ws), N + 4};
     L.init(q.t);
     __syncthreads();
     auto plane = [&](long long b, int k) -> const float* {
@@ -769,7 +770,7 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
                                    g.smem, st>>>(tws, a, g.G, vec_ok(a.out_a, a.out_dist),
                                                  g.ring);
         } else {
-            if constexpr (N >= 512) {
+            if constexpr (N >= 64) {
                 if (a.land) {
                     if ((e = prep(k2_c2r_land<N>, g.smem)) != cudaSuccess) return e;
                     k2_c2r_land<N><<<persistent_grid(k2_c2r_land<N>, g, a.batch), g.threads,
