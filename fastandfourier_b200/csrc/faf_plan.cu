@@ -373,6 +373,14 @@ static bool ring_ok(const float* x, long long dist) {
     return ((unsigned long long)(size_t)x % 16 == 0) && (dist % 4 == 0);
 }
 
+// Real samples landed by bulk copy and read as float2 pairs (k2_r2c_land):
+// every transform start 8-byte aligned.  FAF_CUDA_NO_STAGING=1: direct loads.
+static bool pairs_ok(const float* x, long long dist) {
+    const char* env = std::getenv("FAF_CUDA_NO_STAGING");
+    if (env && env[0] == '1') return false;
+    return ((unsigned long long)(size_t)x % 8 == 0) && (dist % 2 == 0);
+}
+
 // Bulk copies of a C2C input into the workspace (k2_c2c_land and the
 // tensor-core kernels): any plane alignment and distance; interleaved pairs
 // 8-byte aligned (as the direct loads need).  FAF_CUDA_NO_STAGING=1: direct
@@ -1109,10 +1117,19 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
     const int slots = p->inner.n + 1;
     if (p->inner.ct_log2) {
         const RealShape sh = r2c_shape(p->inner.ct_log2);
-        return fafk::launch_pot2(
-            1, p->inner.ct_log2, p->inner.d_tws, &a,
-            geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? sh.ring : 0, sh.threads),
-            st);
+        fafk::Geometry g =
+            geometry_ct(p->inner, slots, batch, ring_ok(x, in_dist) ? sh.ring : 0, sh.threads);
+        // groups narrower than a warp take no ring.  At inner length 256
+        // (n = 512) their samples land in the group's workspace
+        // (k2_r2c_land): 3849 -> 4602 GB/s on B200 (2^25 samples per launch).
+        // Shorter lengths measured no gain (n = 64: 1498 against 1501; 128:
+        // 2128 against 2191; 256: 3152 against 3330) and keep the direct loads.
+        const int T = p->inner.n / 16;
+        if (p->inner.ct_log2 == 8 && pairs_ok(x, in_dist)) {
+            a.land = 1;
+            cap_land_groups(g, T);
+        }
+        return fafk::launch_pot2(1, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
     }
     return fafk::launch_r2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
                             p->inner.d_tw, a, st);

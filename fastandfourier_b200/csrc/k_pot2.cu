@@ -257,6 +257,75 @@ __global__ void __launch_bounds__(1024) k2_r2c(const float2* __restrict__ tws, c
     if constexpr (RING) fafct::ring_drain(R);
 }
 
+// R2C of power-of-two inner lengths 32 to 256 (n = 64 to 512; launched at 256,
+// where it measured faster than the direct loads), whose groups are narrower
+// than a warp and take no ring: each transform's samples land in
+// its group's workspace by bulk copy (every transform start 8-byte aligned,
+// so they read as float2 pairs), issued for the group's next transform once
+// the group has read the workspace.  With up to kLandMaxGroups groups per CTA
+// one group's copy overlaps the others' compute.
+template <int N>
+__global__ void __launch_bounds__(1024) k2_r2c_land(const float2* __restrict__ tws,
+                                                    const RealArgs a, int G) {
+    static_assert(N >= 32 && P2<N, kRO>::T < 32, "sub-warp groups of at least two stages");
+    extern __shared__ float4 smem4[];
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    CtGroup<N, kRO> q(sm, N + 1, tws);
+    using Ctl = LandCtlN<kLandMaxGroups>;
+    __shared__ Ctl ctl;
+    const SmemC mid{q.ws};
+    const int fpe = a.interleaved ? 2 : 1;
+    LandPlanes<Ctl> L{&ctl, q.g, reinterpret_cast<float*>(q.ws), 0};
+    L.init(q.t);
+    __syncthreads();
+    const long long stride = (long long)gridDim.x * G;
+    long long b = (long long)blockIdx.x * G + q.g;
+    if (q.t == 0 && b < a.batch) L.issue(a.in_a + b * a.in_dist, nullptr, N);
+    for (; b - q.g < a.batch; b += stride) {  // the same trip count for every group
+        const bool live = b < a.batch;
+        const long long bi = live ? b : 0;
+        if (live) L.wait(a.err, q.t);
+        const LandSrc src{L.first(a.in_a + bi * a.in_dist), nullptr, 1, 1.0f};
+        const long long oo = bi * a.out_dist * fpe;
+        if constexpr (fafct::LastPairs<N, kRO>::ok) {
+            // last stage fused with the post-pass
+            fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, src, q.sync);
+            if (live) {
+                const float sc = a.scale;
+                const float2* __restrict__ stw = a.stw;
+                auto post = [&](const auto& out) {
+                    fafct::ct_last_pairs<N, kTw<N, kRO>, kRO, kR2cSel<N, false>>(
+                        q.t, q.ws, q.tw,
+                        [&](cf z) {
+                            out.put(0, (z.x + z.y) * sc, 0.f);
+                            out.put(N, (z.x - z.y) * sc, 0.f);
+                        },
+                        [&](int k, cf zk, cf zn) {
+                            cf Xk, Xnk;
+                            r2c_pair(zk, zn, __ldg(&stw[k - 1]), Xk, Xnk);
+                            if (k != N - k) out.put(k, Xk.x * sc, Xk.y * sc);
+                            out.put(N - k, Xnk.x * sc, Xnk.y * sc);
+                        });
+                };
+                if (a.interleaved)
+                    post(HermInter{reinterpret_cast<float2*>(a.out_a + oo)});
+                else
+                    post(HermSplit{a.out_a + oo, a.out_b + oo});
+            }
+        } else {
+            ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, src, mid, q.sync);
+            if (live) {
+                HermSink out{a.out_a + oo, a.interleaved ? nullptr : a.out_b + oo, a.interleaved};
+                ct_r2c_post<N>(q.t, mid, a.stw, out, a.scale);
+            }
+        }
+        q.sync();  // the whole group has read the workspace
+        const long long bn = b + stride;
+        if (q.t == 0 && bn < a.batch) L.issue(a.in_a + bn * a.in_dist, nullptr, N);
+    }
+    L.drain(q.t);
+}
+
 // RING: each frame's first `win` samples land in the ring by bulk copy
 // (frame starts 16-byte aligned, win a multiple of 4), the window is staged in
 // shared memory behind the ring; otherwise the first stage loads both.
@@ -751,6 +820,14 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     }
     case 1: {
         const RealArgs& a = *(const RealArgs*)args;
+        if constexpr (N == 256) {
+            if (a.land) {
+                if ((e = prep(k2_r2c_land<N>, g.smem)) != cudaSuccess) return e;
+                k2_r2c_land<N><<<persistent_grid(k2_r2c_land<N>, g, a.batch), g.threads, g.smem,
+                                 st>>>(tws, a, g.G);
+                break;
+            }
+        }
         if (kRingN<N> && g.ring) {
             if ((e = prep(k2_r2c<N, kRingN<N>>, g.smem)) != cudaSuccess) return e;
             k2_r2c<N, kRingN<N>><<<persistent_grid(k2_r2c<N, kRingN<N>>, g, a.batch), g.threads,

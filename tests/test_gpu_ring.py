@@ -56,6 +56,58 @@ def test_r2c_ring_and_direct_distances(cuda, dist_pad):
     assert t.wait_status() == 0
 
 
+@pytest.mark.parametrize("n", [64, 128, 256, 512])
+@pytest.mark.parametrize("batch", [1, 5, 1187, 20000 + 3])
+@pytest.mark.parametrize("inter", [False, True])
+def test_r2c_landed_short_lengths_match_direct_loads(cuda, monkeypatch, n, batch, inter):
+    """R2C of 512 samples (groups narrower than a warp) lands each
+    transform's samples in its group's workspace: bit-identical to the direct
+    loads and equal to FP64 within the tolerance, for split and interleaved
+    spectra; 64 to 256 samples take the direct loads both times."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    x = seeded(n + batch).standard_normal((batch, n)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    nb = n // 2 + 1
+
+    def run():
+        t = F.Transform.rfft(n, layout=F.L_INTERLEAVED if inter else F.L_DEFAULT)
+        if inter:
+            y = t.r2c(xd).cpu().numpy().reshape(batch, nb, 2)
+            got = y[..., 0] + 1j * y[..., 1]
+        else:
+            Xr, Xi = t.r2c(xd)
+            got = Xr.cpu().numpy() + 1j * Xi.cpu().numpy()
+        assert t.wait_status() == 0
+        return got
+
+    got = run()
+    assert rel(got, np.fft.rfft(x.astype(np.float64), axis=-1)) <= REL_L2_TOL
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    assert np.array_equal(got, run())
+
+
+@pytest.mark.parametrize("dist_pad", [1, 2, 3])
+def test_r2c_short_odd_distances(cuda, dist_pad):
+    """Distances of odd floats (transform starts 4-byte aligned) take the
+    direct loads; even ones land.  Both match FP64."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n, batch = 512, 999
+    dist = n + dist_pad
+    x = seeded(dist).standard_normal((batch, n)).astype(np.float32)
+    buf = _strided(torch, x, dist)
+    nb = n // 2 + 1
+    Xr = torch.empty(batch * nb, device="cuda")
+    Xi = torch.empty(batch * nb, device="cuda")
+    t = F.Transform.rfft(n)
+    t.execute_batched(F._buf(Xr, Xi, nb, F.L_HERMITIAN), F._buf(buf, None, n, F.L_REAL), batch,
+                      in_dist=dist, out_dist=nb)
+    got = Xr.cpu().numpy().reshape(batch, nb) + 1j * Xi.cpu().numpy().reshape(batch, nb)
+    assert rel(got, np.fft.rfft(x.astype(np.float64), axis=-1)) <= REL_L2_TOL
+    assert t.wait_status() == 0
+
+
 @pytest.mark.parametrize("batch", [3, 640, 8192 + 7])
 def test_pipeline_ring_batches(cuda, batch):
     import fastandfourier_b200 as F
