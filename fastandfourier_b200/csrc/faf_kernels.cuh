@@ -107,6 +107,9 @@ struct RealArgs {  // R2C / C2R / pipeline / STFT
     // ring: the spectrum and the super-twiddles are copied to shared memory
     // behind the ring slots (pipe_table_bytes(N) of them)
     int stage_tables = 0;
+    // R2C of inner lengths 32 to 128: spectra staged in shared memory behind
+    // the workspaces (N + 1 float2 per group) and written row by row
+    int stage_out = 0;
 };
 
 // Shared-memory bytes of the staged pipeline tables for inner length N: the

@@ -315,7 +315,9 @@ fafk::Geometry geometry(const FftSize& s, int slots, int extra_floats, long long
 // CTA width and input-ring slots of the R2C and pipeline kernels by inner
 // length (2^ct_log2).  Measured on B200 (2^25 samples per launch, 40-launch
 // event loops, GB/s):
-//   R2C n = 256 / 512: 256 threads 3245 / 3582, 1024 threads 2857 / 3377
+//   R2C n = 64 / 128 / 256 (spectra staged, k2_r2c_small): 128 threads
+//     2743 / 3032 / 3486, 256 threads 2534 / 2958 / 3457, 1024 threads
+//     2069 / 2394 / 2854; n = 512: 256 threads 3582, 1024 threads 3377
 //     (no ring below inner length 512); n = 2048: 256 threads with 2 slots
 //     4848, 1024 threads with 8 slots 4486; n = 4096 and up: 1024 threads
 //     with 8 slots (5012 at 4096; 256 or 512 threads 3200-4420).
@@ -330,7 +332,8 @@ struct RealShape {
     int threads, ring;
 };
 static RealShape r2c_shape(int ct_log2) {
-    if (ct_log2 == 7 || ct_log2 == 8 || ct_log2 == 10) return {256, 2};
+    if (ct_log2 >= 5 && ct_log2 <= 7) return {128, 2};
+    if (ct_log2 == 8 || ct_log2 == 10) return {256, 2};
     return {1024, fafct::kRingMax};
 }
 static RealShape pipe_shape(int ct_log2) {
@@ -371,6 +374,12 @@ static bool ring_ok(const float* x, long long dist) {
     const char* env = std::getenv("FAF_CUDA_NO_STAGING");
     if (env && env[0] == '1') return false;
     return ((unsigned long long)(size_t)x % 16 == 0) && (dist % 4 == 0);
+}
+
+// FAF_CUDA_NO_STAGING=1 turns off every landing and staging path.
+static bool staging_on() {
+    const char* env = std::getenv("FAF_CUDA_NO_STAGING");
+    return !(env && env[0] == '1');
 }
 
 // Real samples landed by bulk copy and read as float2 pairs (k2_r2c_land):
@@ -1128,6 +1137,19 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
         if (p->inner.ct_log2 == 8 && pairs_ok(x, in_dist)) {
             a.land = 1;
             cap_land_groups(g, T);
+        }
+        // inner lengths 32 to 128: spectra staged behind the workspaces and
+        // written row by row (k2_r2c_small)
+        if (p->inner.ct_log2 >= 5 && p->inner.ct_log2 <= 7 && staging_on()) {
+            a.stage_out = 1;
+            const size_t per = g.smem / g.G;
+            const size_t row = (size_t)(p->inner.n + 1) * sizeof(float2);
+            const size_t table = fafk::pot2_table_smem(p->inner.ct_log2, p->inner.ct_ord);
+            int G = g.G;
+            while (G > 1 && (size_t)G * (per + row) + table > kMaxSmem) G--;
+            g.G = G;
+            g.threads = G * T;
+            g.smem = (size_t)G * (per + row);
         }
         return fafk::launch_pot2(1, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
     }

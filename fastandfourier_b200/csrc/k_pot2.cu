@@ -136,9 +136,9 @@ __global__ void __launch_bounds__(1024) k2_c2c_land(const float2* __restrict__ t
 }
 
 // Post-pass over bin pairs after the forward FFT left Z in the workspace.
-template <int N>
+template <int N, class Out>
 __device__ __forceinline__ void ct_r2c_post(int t, const SmemC& mid,
-                                            const float2* __restrict__ stw, const HermSink& out,
+                                            const float2* __restrict__ stw, const Out& out,
                                             float scale) {
     constexpr int nc = N;
     for (int k = t; k <= nc / 2; k += P2<N>::T) {
@@ -324,6 +324,73 @@ __global__ void __launch_bounds__(1024) k2_r2c_land(const float2* __restrict__ t
         if (q.t == 0 && bn < a.batch) L.issue(a.in_a + bn * a.in_dist, nullptr, N);
     }
     L.drain(q.t);
+}
+
+// One transform's spectrum staged in shared memory (bin k at p[k]).
+struct HermStage {
+    float2* p;
+    __device__ __forceinline__ void put(int k, float r, float i) const {
+        p[k] = make_float2(r, i);
+    }
+};
+
+// R2C of power-of-two inner lengths 32 to 128 (n = 64 to 256).  Their groups
+// are 2 to 8 threads, so each spectrum store of k2_r2c writes bins of 4 to 16
+// transforms and uses little of each sector it touches.  Here every group
+// puts its bins in a staging row behind the workspaces, and the CTA then
+// writes its G consecutive transforms' spectra row after row, consecutive
+// threads on consecutive bins.
+template <int N>
+__global__ void __launch_bounds__(1024) k2_r2c_small(const float2* __restrict__ tws,
+                                                     const RealArgs a, int G, bool vec) {
+    static_assert(N >= 32 && P2<N, kRO>::T < 32, "sub-warp groups");
+    constexpr int NB = N + 1;
+    extern __shared__ float4 smem4[];
+    float2* sm = reinterpret_cast<float2*>(smem4);
+    CtGroup<N, kRO> q(sm, N + 1, tws);
+    float2* stg = ring_base<N, kRO>(sm, G, N + 1);
+    const SmemC mid{q.ws};
+    const HermStage out{stg + q.g * NB};
+    const float sc = a.scale;
+    const float2* __restrict__ stw = a.stw;
+    CT_FOR_GROUPS(G, a.batch) {
+        const long long b0 = grp_ * G;
+        const long long b = b0 + q.g;
+        const bool live = b < a.batch;
+        const RealPairSrc src{a.in_a + (live ? b : 0) * a.in_dist, live, vec};
+        if constexpr (fafct::LastPairs<N, kRO>::ok) {
+            fafct::ct_fft_but_last<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, src, q.sync);
+            fafct::ct_last_pairs<N, kTw<N, kRO>, kRO, kR2cSel<N, false>>(
+                q.t, q.ws, q.tw,
+                [&](cf z) {
+                    out.put(0, (z.x + z.y) * sc, 0.f);
+                    out.put(N, (z.x - z.y) * sc, 0.f);
+                },
+                [&](int k, cf zk, cf zn) {
+                    cf Xk, Xnk;
+                    r2c_pair(zk, zn, __ldg(&stw[k - 1]), Xk, Xnk);
+                    if (k != N - k) out.put(k, Xk.x * sc, Xk.y * sc);
+                    out.put(N - k, Xnk.x * sc, Xnk.y * sc);
+                });
+        } else {
+            ct_fft<N, kTw<N, kRO>, kRO>(q.t, q.ws, q.tw, src, mid, q.sync);
+            ct_r2c_post<N>(q.t, mid, stw, out, sc);
+        }
+        __syncthreads();  // every group's bins are staged
+        const int nl = (int)min((long long)G, a.batch - b0);
+        for (int i = threadIdx.x; i < nl * NB; i += blockDim.x) {
+            const int j = i / NB, k = i - j * NB;
+            const float2 v = stg[i];
+            const long long o = (b0 + j) * a.out_dist + k;
+            if (a.interleaved) {
+                __stcs(reinterpret_cast<float2*>(a.out_a) + o, v);
+            } else {
+                __stcs(a.out_a + o, v.x);
+                __stcs(a.out_b + o, v.y);
+            }
+        }
+        __syncthreads();  // the staging rows are free for the next round
+    }
 }
 
 // RING: each frame's first `win` samples land in the ring by bulk copy
@@ -820,6 +887,14 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     }
     case 1: {
         const RealArgs& a = *(const RealArgs*)args;
+        if constexpr (N >= 32 && N <= 128) {
+            if (a.stage_out) {
+                if ((e = prep(k2_r2c_small<N>, g.smem)) != cudaSuccess) return e;
+                k2_r2c_small<N><<<persistent_grid(k2_r2c_small<N>, g, a.batch), g.threads,
+                                  g.smem, st>>>(tws, a, g.G, vec_ok(a.in_a, a.in_dist));
+                break;
+            }
+        }
         if constexpr (N == 256) {
             if (a.land) {
                 if ((e = prep(k2_r2c_land<N>, g.smem)) != cudaSuccess) return e;

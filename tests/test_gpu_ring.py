@@ -60,10 +60,11 @@ def test_r2c_ring_and_direct_distances(cuda, dist_pad):
 @pytest.mark.parametrize("batch", [1, 5, 1187, 20000 + 3])
 @pytest.mark.parametrize("inter", [False, True])
 def test_r2c_landed_short_lengths_match_direct_loads(cuda, monkeypatch, n, batch, inter):
-    """R2C of 512 samples (groups narrower than a warp) lands each
-    transform's samples in its group's workspace: bit-identical to the direct
-    loads and equal to FP64 within the tolerance, for split and interleaved
-    spectra; 64 to 256 samples take the direct loads both times."""
+    """Groups narrower than a warp: R2C of 512 samples lands each
+    transform's samples in its group's workspace, and 64 to 256 samples stage
+    their spectra in shared memory and write them row by row.  Both are
+    bit-identical to k2_r2c's direct loads and stores and equal FP64 within
+    the tolerance, for split and interleaved spectra."""
     import fastandfourier_b200 as F
     torch = cuda
     x = seeded(n + batch).standard_normal((batch, n)).astype(np.float32)
@@ -87,24 +88,30 @@ def test_r2c_landed_short_lengths_match_direct_loads(cuda, monkeypatch, n, batch
     assert np.array_equal(got, run())
 
 
-@pytest.mark.parametrize("dist_pad", [1, 2, 3])
-def test_r2c_short_odd_distances(cuda, dist_pad):
-    """Distances of odd floats (transform starts 4-byte aligned) take the
-    direct loads; even ones land.  Both match FP64."""
+@pytest.mark.parametrize("n", [64, 128, 512])
+@pytest.mark.parametrize("dist_pad,out_pad", [(1, 0), (2, 3), (3, 1)])
+def test_r2c_short_odd_distances(cuda, n, dist_pad, out_pad):
+    """Input distances of odd floats (transform starts 4-byte aligned) take
+    the direct loads at 512 samples; even ones land.  The staged spectra of
+    64 and 128 samples go to rows `nb + out_pad` apart.  All match FP64."""
     import fastandfourier_b200 as F
     torch = cuda
-    n, batch = 512, 999
+    batch = 999
     dist = n + dist_pad
-    x = seeded(dist).standard_normal((batch, n)).astype(np.float32)
+    x = seeded(dist + n).standard_normal((batch, n)).astype(np.float32)
     buf = _strided(torch, x, dist)
     nb = n // 2 + 1
-    Xr = torch.empty(batch * nb, device="cuda")
-    Xi = torch.empty(batch * nb, device="cuda")
+    od = nb + out_pad
+    Xr = torch.full((batch * od,), 7.0, device="cuda")
+    Xi = torch.full((batch * od,), 7.0, device="cuda")
     t = F.Transform.rfft(n)
     t.execute_batched(F._buf(Xr, Xi, nb, F.L_HERMITIAN), F._buf(buf, None, n, F.L_REAL), batch,
-                      in_dist=dist, out_dist=nb)
-    got = Xr.cpu().numpy().reshape(batch, nb) + 1j * Xi.cpu().numpy().reshape(batch, nb)
+                      in_dist=dist, out_dist=od)
+    yr = Xr.cpu().numpy().reshape(batch, od)
+    yi = Xi.cpu().numpy().reshape(batch, od)
+    got = yr[:, :nb] + 1j * yi[:, :nb]
     assert rel(got, np.fft.rfft(x.astype(np.float64), axis=-1)) <= REL_L2_TOL
+    assert np.all(yr[:, nb:] == 7.0) and np.all(yi[:, nb:] == 7.0)  # gaps untouched
     assert t.wait_status() == 0
 
 
