@@ -355,17 +355,22 @@ static void cap_land_groups(fafk::Geometry& g, int T) {
     g.threads = g.G * T;
 }
 
-// Input ring slots and CTA width of the STFT kernel (FAF_CUDA_STFT_RING and
-// FAF_CUDA_CTA_THREADS override).  Measured on B200 (Hann 1024 / hop 256,
-// 64 x 2^18 samples, 200-step event loops): 384 threads (12 groups) with 8
-// slots 105.6 us; 512 threads (15 groups) with 8 slots 106.7, with 4 slots
-// 118.9; 256 threads with 6 slots 106.8.  With 4 slots behind 12 or 15
-// groups, groups wait for a free slot.
-static int stft_ring() {
-    const char* env = std::getenv("FAF_CUDA_STFT_RING");
-    return env ? atoi(env) : 8;
+// CTA width and input-ring slots of the STFT kernel by inner length
+// (FAF_CUDA_CTA_THREADS and FAF_CUDA_STFT_RING override).  Measured on B200
+// (Hann window of n, hop n / 4, 64 x 2^18 samples, GB/s): n = 256: 384
+// threads with 8 slots 2204, 512 with 4 2032; n = 512: 256 with 8 2907, 384
+// with 8 2772, 512 with 4 2862; n = 1024: 384 with 8 3177 (200-step bench
+// line 3156-3162), 512 with 4 2813 (the ring's groups slept waiting for a
+// slot); n = 2048: 384 with 4 2923, with 8 2511; n = 4096: 1024 with 8 2790,
+// 512 with 4 2246; n = 8192: 1024 with 8 2049, 512 with 4 1759.
+static RealShape stft_shape(int ct_log2) {
+    RealShape sh{1024, 8};
+    if (ct_log2 <= 7 || ct_log2 == 9) sh = {384, 8};
+    else if (ct_log2 == 8) sh = {256, 8};
+    else if (ct_log2 == 10) sh = {384, 4};
+    if (const char* env = std::getenv("FAF_CUDA_STFT_RING")) sh.ring = atoi(env);
+    return sh;
 }
-constexpr int kStftThreads = 384;
 
 // Bulk copies of a real input into the ring need every transform start
 // 16-byte aligned: base address and distance (floats) a multiple of 4.
@@ -1318,10 +1323,11 @@ cudaError_t exec_stft(DevicePlan* p, const float* x, float* Xr, float* Xi, long 
     // frames land by bulk copy when every frame start is 16-byte aligned and
     // the window is a whole number of 16-byte units
     const bool ring = ring_ok(x, sig_len) && a.hop % 4 == 0 && a.win % 4 == 0;
+    const RealShape sh = stft_shape(p->inner.ct_log2);
     if (p->inner.ct_log2)
         return fafk::launch_pot2(
             4, p->inner.ct_log2, p->inner.d_tws, &a,
-            geometry_ct(p->inner, slots, batch, ring ? stft_ring() : 0, kStftThreads,
+            geometry_ct(p->inner, slots, batch, ring ? sh.ring : 0, sh.threads,
                         ((size_t)a.win * sizeof(float) + 15) & ~(size_t)15),
             st);
     return fafk::launch_stft(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
