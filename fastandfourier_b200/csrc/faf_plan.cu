@@ -1267,10 +1267,16 @@ cudaError_t exec_cwt(DevicePlan* p, const float* x, float* W, long long batch, l
         const int N = p->inner.n;
         if (p->inner.ct_log2 && !p->large && xd == fafk::cwt_slot_x(N) &&
             p->psi_dist == fafk::cwt_slot_psi(N) && ring_ok(spec, 2 * xd)) {
-            // spectrum and bank row of every row transform land in the ring
+            // spectrum and bank row of every row transform land in the ring.
+            // 1024-thread CTAs up to n = 4096, 512 beyond: measured on B200
+            // (60 rows, 2^20 samples of signals, GB/s at 1024 / 512 threads
+            // with 8 slots) n = 1024 2085 / 2089, 2048 2209 / 2150, 4096
+            // 2018 / 1705, 8192 1267 / 1671, 16384 1167 / 1258.
+            const int threads = p->inner.ct_log2 >= 12 ? 512 : 1024;
             e = fafk::launch_pot2(2, p->inner.ct_log2, p->inner.d_tws, &a,
-                                  geometry_ct(p->inner, N + 1, c * p->rows, fafct::kRingMax, 1024,
-                                              0, (size_t)fafk::cwt_slot_f2(N) * sizeof(float2)),
+                                  geometry_ct(p->inner, N + 1, c * p->rows, fafct::kRingMax,
+                                              threads, 0,
+                                              (size_t)fafk::cwt_slot_f2(N) * sizeof(float2)),
                                   st);
         } else {
             e = launch_c2r_args(p, a, c * p->rows, st);
