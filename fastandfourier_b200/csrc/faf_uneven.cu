@@ -492,9 +492,10 @@ cudaError_t enqueue(faf_uneven* u, const Bufs& b, cudaStream_t st) {
         a.scale = P.scale;
         a.sgn = u->inverse ? -1.0f : 1.0f;
         a.offs = P.d_offs;
-        // inputs land by bulk copy (k2_c2c_land from 1024 points, the
-        // radix-16 tensor-core kernel from 8192)
-        a.land = (P.log2n >= (P.plan->tc ? 13 : 10) && fafp::land_ok(b.in_re, false)) ? 1 : 0;
+        // inputs land by bulk copy (k2_c2c_land for every class here, from
+        // 256 points: at most 64 groups of 16 threads fit one CTA, one
+        // mbarrier each; the radix-16 tensor-core kernel from 8192)
+        a.land = (P.log2n >= (P.plan->tc ? 13 : 8) && fafp::land_ok(b.in_re, false)) ? 1 : 0;
         a.err = P.plan->d_wait_err;
         e = P.plan->tc ? fafp::tc_launch(P.plan, a, ss)
                        : fafk::launch_pot2(0, P.log2n, P.tws, &a, P.g, ss);

@@ -55,6 +55,30 @@ def test_uneven_config_lengths(cuda, measure):
     assert orc.rel_l2_complex(pr.cpu().numpy(), pi.cpu().numpy(), gr + 1j * gi) <= REL_L2_TOL
 
 
+def test_uneven_short_power_of_two_classes_land(cuda, monkeypatch):
+    """Power-of-two classes of 256 and 512 points, many transforms each at
+    ragged offsets, land their inputs by bulk copy in the graph: equal to FP64
+    and bit-identical to the direct loads."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    rng = seeded(21)
+    lengths = list(rng.choice([256, 512, 60, 1024], 3000))
+    re, im = ragged(lengths, 22)
+    dr, di = torch.from_numpy(re).cuda(), torch.from_numpy(im).cuda()
+
+    def run():
+        u = F.Uneven(lengths)
+        yr, yi = torch.empty_like(dr), torch.empty_like(di)
+        u.execute(dr, di, yr, yi)
+        return yr.cpu().numpy(), yi.cpu().numpy()
+
+    gr, gi = run()
+    assert check_against_fp64(lengths, re, im, gr, gi) <= REL_L2_TOL
+    monkeypatch.setenv("FAF_CUDA_NO_STAGING", "1")
+    dr2, di2 = run()
+    assert np.array_equal(gr, dr2) and np.array_equal(gi, di2)
+
+
 def test_uneven_matches_single_size_oracle(cuda):
     """Each transform against the oracle restatement of the reference."""
     import fastandfourier_b200 as F
