@@ -34,11 +34,54 @@ __global__ void k_ola(const float* __restrict__ tmp, const float* __restrict__ w
     }
 }
 
+// The same sums with the signal taken from blockIdx.y and the sample index in
+// 32 bits (L < 2^30): k_ola's three 64-bit divisions per sample are most of
+// its instructions.  A power-of-two hop (POW2, lh = log2 hop) divides by a
+// shift.  Frame order and arithmetic are k_ola's, so the results are
+// identical.
+template <bool POW2>
+__global__ void k_ola32(const float* __restrict__ tmp, const float* __restrict__ w, int n,
+                        int win, int hop, int lh, int F, int L, float* __restrict__ y,
+                        long long n_sig) {
+    const unsigned uh = (unsigned)hop;
+    auto div = [&](int v) -> int { return POW2 ? (v >> lh) : (int)((unsigned)v / uh); };
+    for (long long s = blockIdx.y; s < n_sig; s += gridDim.y) {
+        const float* __restrict__ ts = tmp + s * (long long)F * n;
+        float* __restrict__ ys = y + s * (long long)L;
+        for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < L; t += gridDim.x * blockDim.x) {
+            const int f_hi = min(F - 1, div(t));
+            const int f_lo = t >= win ? div(t - win) + 1 : 0;
+            float sum = 0.f, env = 0.f;
+            for (int f = f_lo; f <= f_hi; f++) {
+                const int j = t - f * hop;
+                const float wj = __ldg(&w[j]);
+                sum = fmaf(wj, __ldg(&ts[(long long)f * n + j]), sum);
+                env = fmaf(wj, wj, env);
+            }
+            ys[t] = env > 1e-10f ? sum / env : 0.f;
+        }
+    }
+}
+
 cudaError_t launch_ola(const float* tmp, const float* w, int n, int win, int hop, long long F,
                        long long L, float* y, long long n_sig, cudaStream_t st) {
     const long long total = n_sig * L;
     if (total <= 0) return cudaSuccess;
-    const long long blocks = std::min<long long>((total + 255) / 256, 148LL * 16);
+    constexpr long long kBlocks = 148LL * 16;
+    if (L < (1LL << 30) && F < (1LL << 30)) {
+        const long long gy = std::min<long long>(n_sig, 65535);
+        const long long gx =
+            std::max<long long>(1, std::min<long long>((L + 255) / 256, (kBlocks + gy - 1) / gy));
+        const dim3 grid((unsigned)gx, (unsigned)gy);
+        int lh = 0;
+        while ((1 << lh) < hop) lh++;
+        if ((1 << lh) == hop)
+            k_ola32<true><<<grid, 256, 0, st>>>(tmp, w, n, win, hop, lh, (int)F, (int)L, y, n_sig);
+        else
+            k_ola32<false><<<grid, 256, 0, st>>>(tmp, w, n, win, hop, 0, (int)F, (int)L, y, n_sig);
+        return cudaGetLastError();
+    }
+    const long long blocks = std::min<long long>((total + 255) / 256, kBlocks);
     k_ola<<<(unsigned)blocks, 256, 0, st>>>(tmp, w, n, win, hop, F, L, y, n_sig);
     return cudaGetLastError();
 }

@@ -44,6 +44,28 @@ def test_istft_matches_oracle(cuda, n, win, hop):
     assert np.all(y[:, 0] == 0)  # zero window envelope
 
 
+def test_istft_more_signals_than_grid_rows(cuda):
+    """70000 signals: the overlap-add walks signals along the grid's y axis
+    (at most 65535 rows), so signals past the first 65535 take a second
+    pass.  Every signal matches the FP64 oracle."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n = win = 64
+    hop, frames, n_sig = 16, 9, 70000
+    nb = n // 2 + 1
+    rng = seeded(70000)
+    Xr = rng.standard_normal((n_sig, frames, nb)).astype(np.float32)
+    Xi = rng.standard_normal((n_sig, frames, nb)).astype(np.float32)
+    Xi[..., 0] = 0
+    Xi[..., -1] = 0
+    t = F.Transform.istft(n, win=win, hop=hop)
+    y = t.istft_frames(torch.from_numpy(Xr).cuda(), torch.from_numpy(Xi).cuda()).cpu().numpy()
+    m = well_covered(frames, n, win, hop)
+    for sl in (slice(0, 3), slice(65533, 65538), slice(n_sig - 3, n_sig)):
+        want = orc.istft(Xr[sl], Xi[sl], n, win, hop)
+        assert orc.rel_l2(y[sl][:, m], want[:, m]) <= REL_L2_TOL
+
+
 def test_istft_inverts_stft(cuda):
     import fastandfourier_b200 as F
     torch = cuda
