@@ -37,9 +37,10 @@ __global__ void k_ola(const float* __restrict__ tmp, const float* __restrict__ w
 // The same sums with the signal taken from blockIdx.y and the sample index in
 // 32 bits (L < 2^30): k_ola's three 64-bit divisions per sample are most of
 // its instructions.  A power-of-two hop (POW2, lh = log2 hop) divides by a
-// shift.  Frame order and arithmetic are k_ola's, so the results are
-// identical.
-template <bool POW2>
+// shift.  With MAXF > 0 (every sample covered by at most MAXF frames) the
+// frame loop is unrolled, so a thread's frame loads are in flight together.
+// Frame order and arithmetic are k_ola's, so the results are identical.
+template <bool POW2, int MAXF>
 __global__ void k_ola32(const float* __restrict__ tmp, const float* __restrict__ w, int n,
                         int win, int hop, int lh, int F, int L, float* __restrict__ y,
                         long long n_sig) {
@@ -52,11 +53,31 @@ __global__ void k_ola32(const float* __restrict__ tmp, const float* __restrict__
             const int f_hi = min(F - 1, div(t));
             const int f_lo = t >= win ? div(t - win) + 1 : 0;
             float sum = 0.f, env = 0.f;
-            for (int f = f_lo; f <= f_hi; f++) {
-                const int j = t - f * hop;
-                const float wj = __ldg(&w[j]);
-                sum = fmaf(wj, __ldg(&ts[(long long)f * n + j]), sum);
-                env = fmaf(wj, wj, env);
+            if constexpr (MAXF > 0) {
+                float wv[MAXF], xv[MAXF];
+                // every load in range (frames past f_hi read a clamped
+                // element, whose value the sums below skip)
+#pragma unroll
+                for (int i = 0; i < MAXF; i++) {
+                    const int f = min(f_lo + i, F - 1);
+                    const int j = min(max(t - f * hop, 0), win - 1);
+                    wv[i] = __ldg(&w[j]);
+                    xv[i] = __ldg(&ts[(long long)f * n + j]);
+                }
+#pragma unroll
+                for (int i = 0; i < MAXF; i++) {
+                    if (f_lo + i <= f_hi) {
+                        sum = fmaf(wv[i], xv[i], sum);
+                        env = fmaf(wv[i], wv[i], env);
+                    }
+                }
+            } else {
+                for (int f = f_lo; f <= f_hi; f++) {
+                    const int j = t - f * hop;
+                    const float wj = __ldg(&w[j]);
+                    sum = fmaf(wj, __ldg(&ts[(long long)f * n + j]), sum);
+                    env = fmaf(wj, wj, env);
+                }
             }
             ys[t] = env > 1e-10f ? sum / env : 0.f;
         }
@@ -75,10 +96,19 @@ cudaError_t launch_ola(const float* tmp, const float* w, int n, int win, int hop
         const dim3 grid((unsigned)gx, (unsigned)gy);
         int lh = 0;
         while ((1 << lh) < hop) lh++;
-        if ((1 << lh) == hop)
-            k_ola32<true><<<grid, 256, 0, st>>>(tmp, w, n, win, hop, lh, (int)F, (int)L, y, n_sig);
+        // frames covering one sample: at most ceil(win / hop)
+        const int cover = (win + hop - 1) / hop;
+        const bool p2 = (1 << lh) == hop;
+        auto go = [&](auto kernel) {
+            kernel<<<grid, 256, 0, st>>>(tmp, w, n, win, hop, p2 ? lh : 0, (int)F, (int)L, y,
+                                         n_sig);
+        };
+        if (cover <= 4)
+            p2 ? go(k_ola32<true, 4>) : go(k_ola32<false, 4>);
+        else if (cover <= 8)
+            p2 ? go(k_ola32<true, 8>) : go(k_ola32<false, 8>);
         else
-            k_ola32<false><<<grid, 256, 0, st>>>(tmp, w, n, win, hop, 0, (int)F, (int)L, y, n_sig);
+            p2 ? go(k_ola32<true, 0>) : go(k_ola32<false, 0>);
         return cudaGetLastError();
     }
     const long long blocks = std::min<long long>((total + 255) / 256, kBlocks);
