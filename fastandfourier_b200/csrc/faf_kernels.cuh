@@ -70,6 +70,10 @@ struct C2CArgs {
     // a wait that ran out
     int land = 0;
     int* err = nullptr;
+    // the landed 64-point kernel without an offset list: outputs staged in
+    // shared memory behind the workspaces (N float2 per group) and written
+    // row by row
+    int stage_out = 0;
 };
 
 // Groups per CTA of a landing C2C kernel whose transforms are narrower than

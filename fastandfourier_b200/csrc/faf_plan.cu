@@ -387,6 +387,26 @@ static bool staging_on() {
     return !(env && env[0] == '1');
 }
 
+// Outputs staged in shared memory and written row by row (k2_r2c_small,
+// k2_c2c_land<N, true>); FAF_CUDA_STAGE_OUT=0 turns that off alone.
+static bool stage_out_on() {
+    const char* env = std::getenv("FAF_CUDA_STAGE_OUT");
+    return staging_on() && !(env && env[0] == '0');
+}
+
+// A staging row of `row` bytes per group behind the workspaces (`g` holds
+// workspaces only: no ring at these lengths); fewer groups where the rows do
+// not fit.
+static void add_stage_rows(fafk::Geometry& g, const FftSize& s, size_t row) {
+    const size_t per = g.smem / g.G;
+    const size_t table = fafk::pot2_table_smem(s.ct_log2, s.ct_ord);
+    int G = g.G;
+    while (G > 1 && (size_t)G * (per + row) + table > kMaxSmem) G--;
+    g.G = G;
+    g.threads = G * (s.n / 16);
+    g.smem = (size_t)G * (per + row);
+}
+
 // Real samples landed by bulk copy and read as float2 pairs (k2_r2c_land):
 // every transform start 8-byte aligned.  FAF_CUDA_NO_STAGING=1: direct loads.
 static bool pairs_ok(const float* x, long long dist) {
@@ -1083,8 +1103,17 @@ cudaError_t exec_c2c(DevicePlan* p, const float* in_re, const float* in_im, floa
         const int slots = p->inner.n;
         if (p->tc) return tc_launch(p, a, st);
         if (p->inner.ct_log2) {
-            fafk::Geometry g = geometry_ct(p->inner, slots, batch);
+            // 64 points: outputs staged and written row by row, in 128-thread
+            // CTAs.  Measured on B200 (2^25 points per launch): 3685 against
+            // 3389 GB/s for the direct stores; at 128 and 256 points staging
+            // measured slower (4509 against 5855, 4500 against 5763).
+            const bool stg = a.land && p->inner.ct_log2 == 6 && stage_out_on();
+            fafk::Geometry g = geometry_ct(p->inner, slots, batch, 0, stg ? 128 : 0);
             if (a.land) cap_land_groups(g, p->inner.n / 16);
+            if (stg) {
+                a.stage_out = 1;
+                add_stage_rows(g, p->inner, (size_t)p->inner.n * sizeof(float2));
+            }
             return fafk::launch_pot2(0, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
         }
         return fafk::launch_c2c(p->inner.shape(slots), geometry(p->inner, slots, 0, batch),
@@ -1145,16 +1174,9 @@ cudaError_t exec_r2c(DevicePlan* p, const float* x, float* Xr, float* Xi, long l
         }
         // inner lengths 32 to 128: spectra staged behind the workspaces and
         // written row by row (k2_r2c_small)
-        if (p->inner.ct_log2 >= 5 && p->inner.ct_log2 <= 7 && staging_on()) {
+        if (p->inner.ct_log2 >= 5 && p->inner.ct_log2 <= 7 && stage_out_on()) {
             a.stage_out = 1;
-            const size_t per = g.smem / g.G;
-            const size_t row = (size_t)(p->inner.n + 1) * sizeof(float2);
-            const size_t table = fafk::pot2_table_smem(p->inner.ct_log2, p->inner.ct_ord);
-            int G = g.G;
-            while (G > 1 && (size_t)G * (per + row) + table > kMaxSmem) G--;
-            g.G = G;
-            g.threads = G * T;
-            g.smem = (size_t)G * (per + row);
+            add_stage_rows(g, p->inner, (size_t)(p->inner.n + 1) * sizeof(float2));
         }
         return fafk::launch_pot2(1, p->inner.ct_log2, p->inner.d_tws, &a, g, st);
     }

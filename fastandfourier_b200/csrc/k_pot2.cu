@@ -99,7 +99,24 @@ __global__ void __launch_bounds__(1024) k2_c2c(const float2* __restrict__ tws, c
 // (faf_land.cuh), issued for the group's next transform as soon as the last
 // stage has read the workspace, so the copy runs during the last stage and
 // the stores.
-template <int N>
+// One transform's output staged in shared memory, scaled and conjugated as
+// SplitSink stores it.
+struct SplitStage {
+    float2* p;
+    float scale;
+    float sgn;
+    static constexpr bool kSmem = false;
+    __device__ __forceinline__ void put(int i, cf v) const {
+        p[i] = make_float2(v.x * scale, sgn * v.y * scale);
+    }
+};
+
+// STG (launched at 64 points, no offset list): the last stage writes a
+// staging row behind the workspaces, and the CTA then writes its G
+// consecutive transforms row after row: groups of 4 threads otherwise store
+// 16 bytes per transform per instruction.  At 128 and 256 points staging
+// measured slower than the direct stores.
+template <int N, bool STG = false>
 __global__ void __launch_bounds__(1024) k2_c2c_land(const float2* __restrict__ tws,
                                                     const C2CArgs a, int G) {
     extern __shared__ float4 smem4[];
@@ -122,15 +139,39 @@ __global__ void __launch_bounds__(1024) k2_c2c_land(const float2* __restrict__ t
         fafct::ct_fft_but_last<N, kTw<N>>(q.t, q.ws, q.tw, L.src(a, bi), q.sync);
         float xr[16], xi[16];
         const long long bn = b + stride;
-        fafct::ct_stage<N, NS - 1, kTw<N>, 0>(
-            xr, xi, q.t, q.tw, SmemC{q.ws},
-            fafct::LastC<SplitSink>{SplitSink{a.out_re + oo,
-                                              a.interleaved ? nullptr : a.out_im + oo, a.scale,
-                                              a.sgn, a.interleaved, live}},
-            q.sync, [&]() {
-                q.sync();  // the whole group has read the workspace
-                if (q.t == 0 && bn < a.batch) L.issue(a, bn);
-            });
+        auto hook = [&]() {
+            q.sync();  // the whole group has read the workspace
+            if (q.t == 0 && bn < a.batch) L.issue(a, bn);
+        };
+        if constexpr (STG) {
+            float2* stg = ring_base<N>(reinterpret_cast<float2*>(smem4), G, N);
+            fafct::ct_stage<N, NS - 1, kTw<N>, 0>(
+                xr, xi, q.t, q.tw, SmemC{q.ws},
+                fafct::LastC<SplitStage>{SplitStage{stg + q.g * N, a.scale, a.sgn}}, q.sync,
+                hook);
+            __syncthreads();  // every group's row is staged
+            const long long b0 = b - q.g;
+            const int nl = (int)min((long long)G, a.batch - b0);
+            for (int i = threadIdx.x; i < nl * N; i += blockDim.x) {
+                const int j = i / N, k = i % N;
+                const float2 v = stg[i];
+                const long long o = (b0 + j) * a.out_dist * fpe;
+                if (a.interleaved) {
+                    __stcs(reinterpret_cast<float2*>(a.out_re + o) + k, v);
+                } else {
+                    __stcs(a.out_re + o + k, v.x);
+                    __stcs(a.out_im + o + k, v.y);
+                }
+            }
+            __syncthreads();  // the staging rows are free for the next round
+        } else {
+            fafct::ct_stage<N, NS - 1, kTw<N>, 0>(
+                xr, xi, q.t, q.tw, SmemC{q.ws},
+                fafct::LastC<SplitSink>{SplitSink{a.out_re + oo,
+                                                  a.interleaved ? nullptr : a.out_im + oo,
+                                                  a.scale, a.sgn, a.interleaved, live}},
+                q.sync, hook);
+        }
     }
     L.drain(q.t);
 }
@@ -873,6 +914,14 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
     switch (kind) {
     case 0: {
         const C2CArgs& a = *(const C2CArgs*)args;
+        if constexpr (N == 64) {
+            if (a.land && a.stage_out) {
+                if ((e = prep(k2_c2c_land<N, true>, g.smem)) != cudaSuccess) return e;
+                k2_c2c_land<N, true><<<persistent_grid(k2_c2c_land<N, true>, g, a.batch),
+                                       g.threads, g.smem, st>>>(tws, a, g.G);
+                break;
+            }
+        }
         if constexpr (N >= 64) {
             if (a.land) {
                 if ((e = prep(k2_c2c_land<N>, g.smem)) != cudaSuccess) return e;

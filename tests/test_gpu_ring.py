@@ -249,6 +249,43 @@ def test_c2c_landed_interleaved_and_unaligned(cuda):
     assert t.wait_status() == 0
 
 
+@pytest.mark.parametrize("n", [64, 128, 256])
+@pytest.mark.parametrize("inverse,inter", [(False, False), (True, False), (False, True)])
+def test_c2c_staged_outputs_match_unstaged(cuda, monkeypatch, n, inverse, inter):
+    """C2C of 64 points stages its outputs in shared memory and writes them
+    row by row: bit-identical to the landed kernel's direct stores
+    (FAF_CUDA_STAGE_OUT=0) and equal to FP64 within the tolerance; 128 and
+    256 points store directly both times."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    re, im, got = _c2c_pair(torch, F, n, 5003, inverse, inter, n + 5)
+    assert rel(got, orc.fp64_c2c(re, im, inverse=inverse)) <= REL_L2_TOL
+    monkeypatch.setenv("FAF_CUDA_STAGE_OUT", "0")
+    _, _, plain = _c2c_pair(torch, F, n, 5003, inverse, inter, n + 5)
+    assert np.array_equal(got, plain)
+
+
+def test_c2c_staged_outputs_row_distance(cuda):
+    """Staged 64-point outputs go to rows `n + 5` apart; the gaps stay."""
+    import fastandfourier_b200 as F
+    torch = cuda
+    n, batch, od = 64, 3001, 69
+    rng = seeded(64)
+    xr = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    xi = rng.uniform(-1, 1, (batch, n)).astype(np.float32)
+    yr = torch.full((batch * od,), 7.0, device="cuda")
+    yi = torch.full((batch * od,), 7.0, device="cuda")
+    t = F.Transform.fft(n)
+    t.execute_batched(F._buf(yr, yi, n, F.L_SPLIT),
+                      F._buf(torch.from_numpy(xr).cuda(), torch.from_numpy(xi).cuda(), n,
+                             F.L_SPLIT), batch, in_dist=n, out_dist=od)
+    a = yr.cpu().numpy().reshape(batch, od)
+    b = yi.cpu().numpy().reshape(batch, od)
+    assert np.all(a[:, n:] == 7.0) and np.all(b[:, n:] == 7.0)
+    assert rel(a[:, :n] + 1j * b[:, :n], orc.fp64_c2c(xr, xi)) <= REL_L2_TOL
+    assert t.wait_status() == 0
+
+
 @pytest.mark.parametrize("n", [64, 128, 512, 1024])
 def test_c2c_landed_interleaved_matches_direct_loads(cuda, monkeypatch, n):
     """Interleaved inputs of sub-warp, one-warp (512-point) and two-warp
