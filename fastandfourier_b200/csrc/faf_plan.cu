@@ -1205,8 +1205,9 @@ cudaError_t exec_c2r(DevicePlan* p, const float* Xr, const float* Xi, float* y, 
     fafk::RealArgs a = real_args(p, batch);
     a.in_a = Xr; a.in_b = Xi; a.out_a = y;
     a.in_dist = in_dist; a.out_dist = out_dist; a.interleaved = interleaved;
-    // bins land by bulk copy from inner length 64 (k2_c2r_land)
-    a.land = (!p->large && p->inner.ct_log2 >= 6 && land_ok(Xr, interleaved)) ? 1 : 0;
+    // bins land by bulk copy from inner length 32 (k2_c2r_land; the 32-point
+    // workspace holds the two landed planes exactly)
+    a.land = (!p->large && p->inner.ct_log2 >= 5 && land_ok(Xr, interleaved)) ? 1 : 0;
     return launch_c2r_args(p, a, batch, st);
 }
 

@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(1024) k2_c2r(const float2* __restrict__ tws, c
     if constexpr (RING) fafct::ring_drain(R);
 }
 
-// C2R of power-of-two inner lengths from 64 points (no filter rows): each
+// C2R of power-of-two inner lengths from 32 points (no filter rows): each
 // transform's bins land in its group's workspace by bulk copy (faf_land.cuh),
 // issued for the group's next transform once the last stage has read the
 // workspace.  The pre-pass reads every bin pair the thread owns into
@@ -971,7 +971,7 @@ static cudaError_t ct_launch(int kind, const float2* tws, const void* args, Geom
                                    g.smem, st>>>(tws, a, g.G, vec_ok(a.out_a, a.out_dist),
                                                  g.ring);
         } else {
-            if constexpr (N >= 64) {
+            if constexpr (N >= 32) {
                 if (a.land) {
                     if ((e = prep(k2_c2r_land<N>, g.smem)) != cudaSuccess) return e;
                     k2_c2r_land<N><<<persistent_grid(k2_c2r_land<N>, g, a.batch), g.threads,

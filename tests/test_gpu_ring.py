@@ -358,7 +358,7 @@ def test_c2c_landed_inputs_unaligned_outputs(cuda):
     assert t.wait_status() == 0
 
 
-@pytest.mark.parametrize("n", [128, 256, 512, 1024, 4096, 32768])
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024, 4096, 32768])
 @pytest.mark.parametrize("batch", [1, 5, 1187])
 @pytest.mark.parametrize("shift,extra", [(0, 0), (1, 2), (3, 5)])
 def test_c2r_landed_bins_match_direct_loads(cuda, monkeypatch, n, batch, shift, extra):
@@ -395,7 +395,7 @@ def test_c2r_landed_bins_match_direct_loads(cuda, monkeypatch, n, batch, shift, 
     assert np.array_equal(got, run())
 
 
-@pytest.mark.parametrize("n", [128, 512, 1024, 4096])
+@pytest.mark.parametrize("n", [64, 128, 512, 1024, 4096])
 def test_c2r_landed_interleaved_bins(cuda, monkeypatch, n):
     """Interleaved Hermitian input lands as one copy per transform."""
     import fastandfourier_b200 as F
